@@ -1,0 +1,132 @@
+/*
+ * redzone.h -- C-ABI of the B200-native Redzone O(k) in-place stream compaction library.
+ *
+ * The reference (JBontes/redzone) exposes two entry points for this path, both void and both
+ * clobbering the removal list:
+ *   - redzone.hxx:626-627   template<...> __device__ void RemoveFromList_GPUWide(T* List,
+ *                           const int Length, int* Removals, const int RemoveCount,
+ *                           BlockStorage_t<BlockCount>& BlockStore)   (cooperative launch by the
+ *                           caller, T must be 4 bytes, new length implicitly Length-RemoveCount)
+ *   - Redzone_CPU.hxx:150   void redzone_CPU(int* list, int listsize, int* removals,
+ *                           int removecount, int(&times)[4])
+ * This header replaces both with plain-pointer C functions. Every pointer named d_* is a device
+ * pointer owned by the caller; the library owns its scratch. Nothing here aborts or traps:
+ * errors come back as rz_status codes.
+ *
+ * Result contract (identical to the reference on the surviving prefix):
+ *   cut = n - k. For i in [0,k): dest = idx[i], src = cut + i. A source is valid iff src is not
+ *   itself in idx; a destination is valid iff dest < cut. Valid/valid pairs move data[src] to
+ *   data[dest]. Valid destinations without a valid source form the destination-orphan list D
+ *   (in i order); valid sources without a valid destination form the source-orphan list S (in i
+ *   order); then data[D[j]] = data[S[j]]. Kept items below cut that are not removed never move.
+ *   The tail [cut, n) is unspecified after the call (this implementation leaves it untouched);
+ *   the index list is never written (the reference clobbers it).
+ */
+#ifndef REDZONE_B200_H
+#define REDZONE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same object as cudaStream_t / CUstream; declared here so the header needs no CUDA headers. */
+typedef struct CUstream_st* rz_stream_t;
+
+typedef struct rz_ctx rz_ctx;
+
+typedef enum rz_status {
+    RZ_OK = 0,
+    RZ_ERR_INVALID_ARG = 1,   /* null pointer, k > n, unsupported element size, misalignment   */
+    RZ_ERR_DUPLICATE = 2,     /* RZ_VALIDATE: an index occurs twice                             */
+    RZ_ERR_OUT_OF_RANGE = 3,  /* RZ_VALIDATE: an index >= n                                     */
+    RZ_ERR_NO_MEMORY = 4,     /* scratch allocation failed or exceeded the context budget       */
+    RZ_ERR_TIMEOUT = 5,       /* a bounded device wait (grid barrier, look-back) gave up        */
+    RZ_ERR_CUDA = 6,          /* a CUDA runtime call failed (see rz_last_cuda_error)           */
+    RZ_ERR_UNSUPPORTED = 7,   /* n >= 2^32, or a feature this build does not provide            */
+    RZ_ERR_BUSY = 8           /* service: admission refused (memory budget or slots exhausted)  */
+} rz_status;
+
+/* Flags for rz_remove / rz_remove_batched. */
+#define RZ_VALIDATE        0x1u  /* check indices for range and duplicates (O(k) extra passes)   */
+#define RZ_SYNC            0x2u  /* synchronise the stream and return the device status          */
+#define RZ_FORCE_PARTITION 0x4u  /* run the O(n) stable partition instead of Redzone             */
+#define RZ_FORCE_BLOCK     0x8u  /* force the single-CTA schedule                                */
+#define RZ_FORCE_GRID      0x10u /* force the grid-wide persistent schedule                      */
+#define RZ_USE_PREDICTOR   0x20u /* let the trained MLP pick the launch configuration            */
+#define RZ_ALLOW_STABLE    0x40u /* caller accepts the partition path's (stable) survivor order  */
+
+/* Launch configuration of the single-list kernels (one entry of the 48-point tuning space). */
+typedef struct rz_launch_cfg {
+    int32_t block;          /* threads per CTA: 128, 256, 512 or 1024                             */
+    int32_t items;          /* items per thread per tile: 1, 2, 4 or 8                            */
+    int32_t ctas_per_sm;    /* grid = ctas_per_sm x SM count (capped by occupancy and tile count) */
+    int32_t use_partition;  /* 1 = O(n) partition path, 0 = Redzone                                */
+} rz_launch_cfg;
+
+/* ---- context ------------------------------------------------------------------------------ */
+int  rz_create(rz_ctx** ctx, int device);
+void rz_destroy(rz_ctx* ctx);
+/* Human-readable name of a status code; returns the number of bytes written (without NUL). */
+int  rz_status_string(int code, char* buf, size_t len);
+/* Text of the last CUDA error seen by this context (empty if none). */
+int  rz_last_cuda_error(const rz_ctx* ctx, char* buf, size_t len);
+/* Synchronise `stream` and return (and clear) the device-side status of calls made on it. */
+int  rz_sync_status(rz_ctx* ctx, rz_stream_t stream);
+/* Number of SMs of the context's device. */
+int  rz_num_sms(const rz_ctx* ctx);
+
+/* ---- single list -------------------------------------------------------------------------- */
+/*
+ * Remove the k distinct positions d_idx[0..k) from d_data[0..n) (elem_bytes in {4,8,16,32}),
+ * in place, asynchronously on `stream`. *new_len (host pointer, may be NULL) receives n-k.
+ * Replaces RemoveFromList_GPUWide (redzone.hxx:626) and redzone_CPU (Redzone_CPU.hxx:150).
+ */
+int rz_remove(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
+              const uint32_t* d_idx, int64_t k, int64_t* new_len, uint32_t flags,
+              rz_stream_t stream);
+
+/* As rz_remove with an explicit launch configuration (used by the autotuner and tests). */
+int rz_remove_cfg(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
+                  const uint32_t* d_idx, int64_t k, const rz_launch_cfg* cfg, uint32_t flags,
+                  rz_stream_t stream);
+
+/*
+ * Host-buffer form of rz_remove: copies h_idx (k entries, ideally pinned) to the device, runs
+ * the removal on the device-resident d_data, synchronises and returns the status. This is the
+ * end-to-end call a host program makes when its removal lists are produced on the CPU.
+ */
+int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
+                       const uint32_t* h_idx, int64_t k, int64_t* new_len, uint32_t flags,
+                       rz_stream_t stream);
+
+/*
+ * O(n) stable partition comparator (mark + single-pass decoupled look-back compaction), in
+ * place. Survivors keep their relative order, as with thrust::remove (Thrust_remove.hxx:15-17)
+ * and InK compact (cuCompactor.cuh:104-141).
+ */
+int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
+                 const uint32_t* d_idx, int64_t k, int64_t* new_len, uint32_t flags,
+                 rz_stream_t stream);
+
+/* The configuration rz_remove would choose for (n, k, elem_bytes) without a predictor. */
+int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
+                   rz_launch_cfg* cfg);
+
+/* ---- diagnostics -------------------------------------------------------------------------- */
+/*
+ * Failure-detection check for the bounded device waits that replace the reference's grid
+ * barriers (cg::grid.sync, redzone.hxx:707-940, and BlockStorage_t::Wait, redzone.hxx:59-80,
+ * which can spin forever): launches one CTA that waits at a barrier nobody else reaches, with
+ * `spin_limit` polls. The wait must give up, record the timeout and return; *status_bits gets
+ * the device status word (bit 2 = timeout). The context's barrier state is reset afterwards.
+ */
+int rz_test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REDZONE_B200_H */

@@ -1,0 +1,163 @@
+"""redzone_b200 -- B200-native Redzone O(k) in-place stream compaction.
+
+Python host mirror of the library's C-ABI (``include/redzone.h``). Arrays are torch CUDA
+tensors used as plain device buffers: the first axis enumerates items, the remaining axes form
+one item (4, 8, 16 or 32 bytes). Removal indices are int32/uint32 tensors of distinct
+positions.
+
+The reference's calls are ``RemoveFromList_GPUWide(List, Length, Removals, RemoveCount,
+BlockStore)`` (redzone.hxx:626) and ``redzone_CPU(list, listsize, removals, removecount,
+times)`` (Redzone_CPU.hxx:150); ``RemoveFromList`` below keeps that argument order and meaning
+and returns the new length instead of leaving it implicit. Unlike the reference it never writes
+the removal list, and it reports errors as ``RedzoneError`` instead of exiting.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _native
+from ._native import (LaunchCfg, RZ_ALLOW_STABLE, RZ_FORCE_BLOCK, RZ_FORCE_GRID, RZ_FORCE_PARTITION,
+                      RZ_SYNC, RZ_USE_PREDICTOR, RZ_VALIDATE, status_string)
+
+__all__ = ["Context", "RedzoneError", "LaunchCfg", "RemoveFromList", "remove", "default_context",
+           "RZ_VALIDATE", "RZ_SYNC", "RZ_FORCE_PARTITION", "RZ_FORCE_BLOCK", "RZ_FORCE_GRID",
+           "RZ_USE_PREDICTOR", "RZ_ALLOW_STABLE", "item_bytes"]
+
+
+class RedzoneError(RuntimeError):
+    def __init__(self, code: int, detail: str = ""):
+        self.code = code
+        msg = f"redzone: {status_string(code)} (status {code})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+def item_bytes(t) -> int:
+    """Bytes per item of a tensor whose first axis enumerates items."""
+    per = t.element_size()
+    for s in t.shape[1:]:
+        per *= int(s)
+    return per
+
+
+def _stream_handle(stream) -> int | None:
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+class Context:
+    """Owns library scratch (bitmap, orphan lists, barrier state) on one device."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        st = _native.lib.rz_create(ctypes.byref(h), device)
+        if st != 0:
+            raise RedzoneError(st, "rz_create")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _native.lib.rz_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            buf = ctypes.create_string_buffer(512)
+            _native.lib.rz_last_cuda_error(self.handle, buf, 512)
+            raise RedzoneError(st, f"{what} {buf.value.decode()}".strip())
+
+    @property
+    def num_sms(self) -> int:
+        return _native.lib.rz_num_sms(self.handle)
+
+    def remove(self, data, idx, flags: int = 0, stream=None) -> int:
+        """In-place Redzone removal; returns the new length (n - k)."""
+        n, k = int(data.shape[0]), int(idx.numel())
+        out = ctypes.c_int64(0)
+        st = _native.lib.rz_remove(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
+                                   ctypes.c_void_p(idx.data_ptr()), k, ctypes.byref(out), flags,
+                                   ctypes.c_void_p(_stream_handle(stream)))
+        self._check(st, "rz_remove")
+        return out.value
+
+    def remove_cfg(self, data, idx, cfg: LaunchCfg, flags: int = 0, stream=None) -> None:
+        n, k = int(data.shape[0]), int(idx.numel())
+        st = _native.lib.rz_remove_cfg(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
+                                       ctypes.c_void_p(idx.data_ptr()), k, ctypes.byref(cfg), flags,
+                                       ctypes.c_void_p(_stream_handle(stream)))
+        self._check(st, "rz_remove_cfg")
+
+    def partition(self, data, idx, flags: int = 0, stream=None) -> int:
+        """O(n) stable partition comparator (survivors keep their order)."""
+        n, k = int(data.shape[0]), int(idx.numel())
+        out = ctypes.c_int64(0)
+        st = _native.lib.rz_partition(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
+                                      ctypes.c_void_p(idx.data_ptr()), k, ctypes.byref(out), flags,
+                                      ctypes.c_void_p(_stream_handle(stream)))
+        self._check(st, "rz_partition")
+        return out.value
+
+    def remove_host_idx(self, data, h_idx, flags: int = 0, stream=None) -> int:
+        """Indices in host memory (numpy or pinned torch CPU tensor); synchronous; returns new length."""
+        n = int(data.shape[0])
+        if hasattr(h_idx, "data_ptr"):
+            ptr, k = h_idx.data_ptr(), int(h_idx.numel())
+        else:
+            ptr, k = h_idx.ctypes.data, int(h_idx.size)
+        out = ctypes.c_int64(0)
+        st = _native.lib.rz_remove_host_idx(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
+                                            ctypes.c_void_p(ptr), k, ctypes.byref(out), flags,
+                                            ctypes.c_void_p(_stream_handle(stream)))
+        self._check(st, "rz_remove_host_idx")
+        return out.value
+
+    def sync_status(self, stream=None) -> int:
+        return _native.lib.rz_sync_status(self.handle, ctypes.c_void_p(_stream_handle(stream)))
+
+    def default_cfg(self, n: int, k: int, w: int) -> LaunchCfg:
+        cfg = LaunchCfg()
+        self._check(_native.lib.rz_default_cfg(self.handle, n, k, w, ctypes.byref(cfg)), "rz_default_cfg")
+        return cfg
+
+    def test_barrier_timeout(self, spin_limit: int) -> int:
+        bits = ctypes.c_uint32(0)
+        self._check(_native.lib.rz_test_barrier_timeout(self.handle, spin_limit, ctypes.byref(bits)),
+                    "rz_test_barrier_timeout")
+        return bits.value
+
+
+_default: dict[int, Context] = {}
+
+
+def default_context(device: int | None = None) -> Context:
+    import torch
+    d = torch.cuda.current_device() if device is None else device
+    if d not in _default:
+        _default[d] = Context(d)
+    return _default[d]
+
+
+def remove(data, idx, flags: int = 0, stream=None) -> int:
+    """Remove the items at positions ``idx`` from ``data`` in place; returns the new length."""
+    return default_context(data.device.index).remove(data, idx, flags, stream)
+
+
+def RemoveFromList(List, Length: int, Removals, RemoveCount: int, flags: int = 0, stream=None) -> int:
+    """Reference-shaped call: RemoveFromList_GPUWide(List, Length, Removals, RemoveCount, ...).
+
+    ``List`` must hold at least ``Length`` items and ``Removals`` at least ``RemoveCount`` indices;
+    only those prefixes are used. Returns ``Length - RemoveCount``.
+    """
+    if RemoveCount > Length or Length > List.shape[0] or RemoveCount > Removals.numel():
+        raise RedzoneError(_native.RZ_ERR_INVALID_ARG, "RemoveFromList sizes")
+    return remove(List[:Length], Removals.reshape(-1)[:RemoveCount], flags, stream)

@@ -1,0 +1,87 @@
+"""ctypes binding of ``include/redzone.h`` (``redzone_b200/_lib/libredzone_b200.so``).
+
+There is no fallback: if the native library is absent, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "_lib" / "libredzone_b200.so"
+HEADERS = sorted((PKG.parent / "include").glob("*.h"))
+
+if not LIB_PATH.exists():
+    raise ImportError(
+        f"redzone_b200 native library not found at {LIB_PATH}; build it with "
+        "`python -c 'import __graft_entry__ as g; g.build()'` or `python redzone_b200/build.py`")
+
+lib = ctypes.CDLL(str(LIB_PATH))
+
+c_vp, c_i32, c_u32, c_i64, c_u64, c_f32 = (ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32,
+                                           ctypes.c_int64, ctypes.c_uint64, ctypes.c_float)
+
+
+class LaunchCfg(ctypes.Structure):
+    _fields_ = [("block", c_i32), ("items", c_i32), ("ctas_per_sm", c_i32), ("use_partition", c_i32)]
+
+    def as_tuple(self):
+        return (self.block, self.items, self.ctas_per_sm, self.use_partition)
+
+    def __repr__(self):
+        return f"LaunchCfg(block={self.block}, items={self.items}, ctas_per_sm={self.ctas_per_sm}, partition={self.use_partition})"
+
+
+# Status codes (rz_status).
+RZ_OK, RZ_ERR_INVALID_ARG, RZ_ERR_DUPLICATE, RZ_ERR_OUT_OF_RANGE, RZ_ERR_NO_MEMORY, \
+    RZ_ERR_TIMEOUT, RZ_ERR_CUDA, RZ_ERR_UNSUPPORTED, RZ_ERR_BUSY = range(9)
+
+# Flags.
+RZ_VALIDATE = 0x1
+RZ_SYNC = 0x2
+RZ_FORCE_PARTITION = 0x4
+RZ_FORCE_BLOCK = 0x8
+RZ_FORCE_GRID = 0x10
+RZ_USE_PREDICTOR = 0x20
+RZ_ALLOW_STABLE = 0x40
+
+
+def _sig(name, restype, argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = argtypes
+    return f
+
+
+_sig("rz_create", c_i32, [ctypes.POINTER(c_vp), c_i32])
+_sig("rz_destroy", None, [c_vp])
+_sig("rz_status_string", c_i32, [c_i32, ctypes.c_char_p, ctypes.c_size_t])
+_sig("rz_last_cuda_error", c_i32, [c_vp, ctypes.c_char_p, ctypes.c_size_t])
+_sig("rz_sync_status", c_i32, [c_vp, c_vp])
+_sig("rz_num_sms", c_i32, [c_vp])
+_sig("rz_remove", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
+_sig("rz_remove_cfg", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(LaunchCfg), c_u32, c_vp])
+_sig("rz_remove_host_idx", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
+_sig("rz_partition", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
+_sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchCfg)])
+_sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
+
+
+def status_string(code: int) -> str:
+    buf = ctypes.create_string_buffer(128)
+    lib.rz_status_string(code, buf, 128)
+    return buf.value.decode()
+
+
+def declared_symbols() -> list[str]:
+    """Every function name declared in include/*.h."""
+    names = []
+    for h in HEADERS:
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(rz_[a-z0-9_]+)\s*\(", text):
+            if m.group(1) not in names:
+                names.append(m.group(1))
+    return names

@@ -1,0 +1,299 @@
+// rz_capi.cpp -- the extern "C" boundary declared in include/redzone.h: context, scratch and
+// dispatch of single-list removals. Kernels live in rz_single.cu; batching, tuning, the learned
+// predictor and the service are in their own translation units.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "rz_internal.h"
+
+namespace rz {
+
+int cuda_fail(rz_ctx* ctx, cudaError_t e, const char* where) {
+    if (ctx) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf), "%s: %s (%s)", where, cudaGetErrorName(e), cudaGetErrorString(e));
+        ctx->last_cuda_error = buf;
+    }
+    return e == cudaErrorMemoryAllocation ? RZ_ERR_NO_MEMORY : RZ_ERR_CUDA;
+}
+
+template <typename T>
+static int grow(rz_ctx* ctx, T*& ptr, size_t& cap, size_t want, bool zero) {
+    if (want <= cap && ptr) return RZ_OK;
+    size_t nc = std::max<size_t>(want, cap * 2);
+    nc = std::max<size_t>(nc, 1024);
+    if (ptr) {
+        RZ_CUDA_TRY(ctx, cudaDeviceSynchronize());
+        RZ_CUDA_TRY(ctx, cudaFree(ptr));
+        ptr = nullptr;
+        cap = 0;
+    }
+    void* p = nullptr;
+    RZ_CUDA_TRY(ctx, cudaMalloc(&p, nc * sizeof(T)));
+    if (zero) RZ_CUDA_TRY(ctx, cudaMemset(p, 0, nc * sizeof(T)));
+    ptr = static_cast<T*>(p);
+    cap = nc;
+    return RZ_OK;
+}
+
+int ensure_lists(rz_ctx* ctx, size_t k) {
+    int st = grow(ctx, ctx->ws.bitmap, ctx->ws.bitmap_words, (k + 31) / 32 + 1, true);
+    if (st != RZ_OK) return st;
+    size_t cap = ctx->ws.list_cap;
+    st = grow(ctx, ctx->ws.dlist, cap, k + 1, false);
+    if (st != RZ_OK) return st;
+    size_t cap2 = ctx->ws.list_cap;
+    st = grow(ctx, ctx->ws.slist, cap2, k + 1, false);
+    if (st != RZ_OK) return st;
+    ctx->ws.list_cap = std::min(cap, cap2);
+    return RZ_OK;
+}
+
+int ensure_seen(rz_ctx* ctx, size_t n) {
+    return grow(ctx, ctx->ws.seen, ctx->ws.seen_words, (n + 31) / 32 + 1, true);
+}
+
+int ensure_partition(rz_ctx* ctx, size_t n, size_t ntiles) {
+    int st = grow(ctx, ctx->ws.part_bits, ctx->ws.part_words, (n + 31) / 32 + 1, true);
+    if (st != RZ_OK) return st;
+    return grow(ctx, ctx->ws.tile_state, ctx->ws.tile_cap, ntiles + 1, true);
+}
+
+int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {
+    if (!ctx->ws.dirty) return RZ_OK;
+    Workspace& w = ctx->ws;
+    if (w.bitmap) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.bitmap, 0, w.bitmap_words * 4, s));
+    if (w.seen) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.seen, 0, w.seen_words * 4, s));
+    if (w.part_bits) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.part_bits, 0, w.part_words * 4, s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.sync, 0, sizeof(GridSync), s));
+    w.dirty = false;
+    return RZ_OK;
+}
+
+int map_status(uint32_t bits) {
+    if (bits & 2u) return RZ_ERR_OUT_OF_RANGE;
+    if (bits & 1u) return RZ_ERR_DUPLICATE;
+    if (bits & 4u) return RZ_ERR_TIMEOUT;
+    if (bits & 8u) return RZ_ERR_DUPLICATE;
+    return RZ_OK;
+}
+
+int read_status(rz_ctx* ctx, cudaStream_t s) {
+    RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    uint32_t h = 0;
+    RZ_CUDA_TRY(ctx, cudaMemcpy(&h, ctx->ws.status, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h) {
+        RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
+        // A failed call may have left barrier state or bitmap bits behind.
+        ctx->ws.dirty = true;
+    }
+    return map_status(h);
+}
+
+static int check_args(const void* data, int64_t n, uint32_t w, const uint32_t* idx, int64_t k) {
+    if (n < 0 || k < 0 || k > n) return RZ_ERR_INVALID_ARG;
+    if (w != 4 && w != 8 && w != 16 && w != 32) return RZ_ERR_INVALID_ARG;
+    if (n >= (int64_t(1) << 32)) return RZ_ERR_UNSUPPORTED;
+    if (k > 0 && (!data || !idx)) return RZ_ERR_INVALID_ARG;
+    const uintptr_t align = w >= 16 ? 16 : w;
+    if (reinterpret_cast<uintptr_t>(data) % align) return RZ_ERR_INVALID_ARG;
+    if (reinterpret_cast<uintptr_t>(idx) % 4) return RZ_ERR_INVALID_ARG;
+    return RZ_OK;
+}
+
+}  // namespace rz
+
+using namespace rz;
+
+extern "C" {
+
+int rz_create(rz_ctx** out, int device) {
+    if (!out) return RZ_ERR_INVALID_ARG;
+    *out = nullptr;
+    rz_ctx* ctx = new (std::nothrow) rz_ctx();
+    if (!ctx) return RZ_ERR_NO_MEMORY;
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        int st = cuda_fail(ctx, e, "cudaSetDevice");
+        delete ctx;
+        return st;
+    }
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) {
+        int st = cuda_fail(ctx, e, "cudaGetDeviceProperties");
+        delete ctx;
+        return st;
+    }
+    ctx->sms = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    Workspace& w = ctx->ws;
+    void* p = nullptr;
+    // status | GridSync | counts | dev_len, one allocation.
+    const size_t bytes = 256 + sizeof(GridSync) + 2 * kMaxGrid * 4 + 256;
+    e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) e = cudaMemset(p, 0, bytes);
+    if (e != cudaSuccess) {
+        int st = cuda_fail(ctx, e, "workspace");
+        delete ctx;
+        return st;
+    }
+    uint8_t* b = static_cast<uint8_t*>(p);
+    w.status = reinterpret_cast<uint32_t*>(b);
+    w.sync = reinterpret_cast<GridSync*>(b + 256);
+    w.counts = reinterpret_cast<uint32_t*>(b + 256 + sizeof(GridSync));
+    w.dev_len = reinterpret_cast<unsigned long long*>(b + 256 + sizeof(GridSync) + 2 * kMaxGrid * 4);
+    *out = ctx;
+    return RZ_OK;
+}
+
+void rz_destroy(rz_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    Workspace& w = ctx->ws;
+    cudaFree(w.status);
+    cudaFree(w.bitmap);
+    cudaFree(w.dlist);
+    cudaFree(w.slist);
+    cudaFree(w.seen);
+    cudaFree(w.part_bits);
+    cudaFree(w.tile_state);
+    cudaFree(w.idx_stage);
+    release_extras(ctx);
+    delete ctx;
+}
+
+int rz_status_string(int code, char* buf, size_t len) {
+    const char* s = "unknown status";
+    switch (code) {
+        case RZ_OK: s = "ok"; break;
+        case RZ_ERR_INVALID_ARG: s = "invalid argument"; break;
+        case RZ_ERR_DUPLICATE: s = "duplicate removal index"; break;
+        case RZ_ERR_OUT_OF_RANGE: s = "removal index out of range"; break;
+        case RZ_ERR_NO_MEMORY: s = "out of device memory"; break;
+        case RZ_ERR_TIMEOUT: s = "bounded device wait timed out"; break;
+        case RZ_ERR_CUDA: s = "CUDA runtime error"; break;
+        case RZ_ERR_UNSUPPORTED: s = "unsupported"; break;
+        case RZ_ERR_BUSY: s = "admission refused"; break;
+        default: break;
+    }
+    if (!buf || len == 0) return int(std::strlen(s));
+    std::snprintf(buf, len, "%s", s);
+    return int(std::strlen(buf));
+}
+
+int rz_last_cuda_error(const rz_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !buf || len == 0) return 0;
+    std::snprintf(buf, len, "%s", ctx->last_cuda_error.c_str());
+    return int(std::strlen(buf));
+}
+
+int rz_sync_status(rz_ctx* ctx, rz_stream_t stream) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return read_status(ctx, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rz_num_sms(const rz_ctx* ctx) { return ctx ? ctx->sms : 0; }
+
+int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes, rz_launch_cfg* cfg) {
+    if (!ctx || !cfg || k < 0 || n < k) return RZ_ERR_INVALID_ARG;
+    if (n >= (int64_t(1) << 32)) return RZ_ERR_UNSUPPORTED;
+    return default_cfg(ctx, uint32_t(n), uint32_t(k), elem_bytes, cfg);
+}
+
+int rz_remove_cfg(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx,
+                  int64_t k, const rz_launch_cfg* cfg, uint32_t flags, rz_stream_t stream) {
+    if (!ctx || !cfg) return RZ_ERR_INVALID_ARG;
+    int st = check_args(d_data, n, elem_bytes, d_idx, k);
+    if (st != RZ_OK) return st;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (k == 0 || k == n) {
+        // Nothing moves (reference: redzone.hxx:651, Redzone_CPU.hxx handles it implicitly).
+        if (flags & RZ_VALIDATE && k > 0) {
+            st = launch_validate(ctx, uint32_t(n), d_idx, uint32_t(k), s);
+            if (st != RZ_OK) return st;
+        }
+        return (flags & RZ_SYNC) ? read_status(ctx, s) : RZ_OK;
+    }
+    if (cfg->use_partition || (flags & RZ_FORCE_PARTITION))
+        st = launch_partition(ctx, d_data, uint32_t(n), elem_bytes, d_idx, uint32_t(k), flags, s, nullptr);
+    else
+        st = launch_redzone(ctx, d_data, uint32_t(n), elem_bytes, d_idx, uint32_t(k), *cfg, flags, s, nullptr);
+    if (st != RZ_OK) return st;
+    return (flags & RZ_SYNC) ? read_status(ctx, s) : RZ_OK;
+}
+
+int rz_remove(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
+              int64_t* new_len, uint32_t flags, rz_stream_t stream) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    int st = check_args(d_data, n, elem_bytes, d_idx, k);
+    if (st != RZ_OK) return st;
+    if (new_len) *new_len = n - k;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    rz_launch_cfg cfg{};
+    bool have = false;
+    if (flags & RZ_USE_PREDICTOR)
+        have = predict_cfg(ctx, uint32_t(n), uint32_t(k), elem_bytes, d_idx,
+                              reinterpret_cast<cudaStream_t>(stream), &cfg);
+    if (!have) have = tuned_cfg(ctx, uint32_t(n), uint32_t(k), elem_bytes, &cfg);
+    if (!have) {
+        st = default_cfg(ctx, uint32_t(n), uint32_t(k), elem_bytes, &cfg);
+        if (st != RZ_OK) return st;
+    }
+    // The partition path reorders survivors; it runs only when the caller allows that order.
+    if (cfg.use_partition && !(flags & RZ_ALLOW_STABLE)) cfg.use_partition = 0;
+    return rz_remove_cfg(ctx, d_data, n, elem_bytes, d_idx, k, &cfg, flags, stream);
+}
+
+int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
+                 int64_t* new_len, uint32_t flags, rz_stream_t stream) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    int st = check_args(d_data, n, elem_bytes, d_idx, k);
+    if (st != RZ_OK) return st;
+    if (new_len) *new_len = n - k;
+    rz_launch_cfg cfg{256, 8, 1, 1};
+    return rz_remove_cfg(ctx, d_data, n, elem_bytes, d_idx, k, &cfg, flags | RZ_FORCE_PARTITION, stream);
+}
+
+int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* h_idx,
+                       int64_t k, int64_t* new_len, uint32_t flags, rz_stream_t stream) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    int st = check_args(d_data, n, elem_bytes, h_idx, k);
+    if (st != RZ_OK) return st;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    st = grow(ctx, ctx->ws.idx_stage, ctx->ws.stage_cap, size_t(k) + 1, false);
+    if (st != RZ_OK) return st;
+    uint32_t* d_stage = ctx->ws.idx_stage;
+    if (k > 0) RZ_CUDA_TRY(ctx, cudaMemcpyAsync(d_stage, h_idx, size_t(k) * 4, cudaMemcpyHostToDevice, s));
+    int64_t nl = 0;
+    st = rz_remove(ctx, d_data, n, elem_bytes, d_stage, k, &nl, flags & ~RZ_SYNC, stream);
+    if (st != RZ_OK) return st;
+    // Read the device-tracked length back: the step's result crosses to the host.
+    unsigned long long dl = 0;
+    if (k > 0 && k < n) {
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(&dl, ctx->ws.dev_len, sizeof(dl), cudaMemcpyDeviceToHost, s));
+    }
+    st = read_status(ctx, s);
+    if (new_len) *new_len = (k > 0 && k < n) ? int64_t(dl) : n - k;
+    return st;
+}
+
+int rz_test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_bits) {
+    if (!ctx || !status_bits) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return test_barrier_timeout(ctx, spin_limit, status_bits);
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// rz_internal.h -- host-side declarations shared by the translation units of the library.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/redzone.h"
+
+namespace rz {
+
+// Generation-barrier state (see grid_barrier in rz_common.cuh): one 128-byte line.
+struct GridSync {
+    uint32_t count;
+    uint32_t gen;
+    uint32_t pad[30];
+};
+
+constexpr int kMaxGrid = 1024;           // upper bound on CTAs of the persistent single-list kernel
+constexpr uint32_t kSpinLimit = 1u << 22;  // polls of a bounded device wait (~0.5-1 s with backoff)
+
+// Library scratch owned by one context. Every buffer is zero where the kernels require it on
+// entry and is left zero on exit (the kernels clear what they set), so no per-call memset is
+// needed; `dirty` forces a full re-zero after a call that ended with a device error.
+struct Workspace {
+    uint32_t* status = nullptr;      // device status word (ST_* bits)
+    GridSync* sync = nullptr;        // generation barrier state
+    uint32_t* counts = nullptr;      // 2 * kMaxGrid per-CTA orphan counts
+    uint32_t* bitmap = nullptr;      // red-zone bitmap, k bits
+    size_t bitmap_words = 0;
+    uint32_t* dlist = nullptr;       // destination orphans (per-CTA regions), k entries
+    uint32_t* slist = nullptr;       // source-orphan positions (per-CTA regions), k entries
+    size_t list_cap = 0;
+    uint32_t* seen = nullptr;        // RZ_VALIDATE: n-bit occupancy map
+    size_t seen_words = 0;
+    uint32_t* part_bits = nullptr;   // partition path: n-bit removal map
+    size_t part_words = 0;
+    unsigned long long* tile_state = nullptr;  // partition path: look-back state + ticket
+    size_t tile_cap = 0;
+    unsigned long long* dev_len = nullptr;     // device copy of the last new length
+    uint32_t* idx_stage = nullptr;   // rz_remove_host_idx: device copy of host indices
+    size_t stage_cap = 0;
+    bool dirty = false;
+};
+
+}  // namespace rz
+
+struct rz_ctx {
+    int device = 0;
+    int sms = 0;
+    size_t smem_optin = 0;
+    rz::Workspace ws;
+    std::string last_cuda_error;
+    std::recursive_mutex mu;
+    void* predictor = nullptr;   // rz::Predictor*, owned (see rz_mlp.cu)
+    void* tune_table = nullptr;  // rz::TuneTable*, owned (see rz_autotune.cpp)
+};
+
+namespace rz {
+
+// Record a CUDA error in the context and map it to RZ_ERR_CUDA.
+int cuda_fail(rz_ctx* ctx, cudaError_t e, const char* where);
+#define RZ_CUDA_TRY(ctx, call)                                   \
+    do {                                                         \
+        cudaError_t _e = (call);                                 \
+        if (_e != cudaSuccess) return ::rz::cuda_fail((ctx), _e, #call); \
+    } while (0)
+
+// Grow-only scratch allocation; returns RZ_OK or an error code.
+int ensure_lists(rz_ctx* ctx, size_t k);
+int ensure_seen(rz_ctx* ctx, size_t n);
+int ensure_partition(rz_ctx* ctx, size_t n, size_t ntiles);
+int reset_if_dirty(rz_ctx* ctx, cudaStream_t s);
+
+// Kernel launchers (rz_single.cu).
+struct LaunchInfo {
+    int grid = 0;
+    int block = 0;
+    int items = 0;
+    int launches = 0;  // kernels launched by this call
+};
+int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx,
+                   uint32_t k, const rz_launch_cfg& cfg, uint32_t flags, cudaStream_t s,
+                   LaunchInfo* info);
+int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx,
+                     uint32_t k, uint32_t flags, cudaStream_t s, LaunchInfo* info);
+int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cudaStream_t s);
+// Largest block size the single-list kernel for (w, items) can launch with.
+int redzone_max_block(int w, int items);
+// CTAs per SM the single-list kernel for (w, items, block) can keep resident.
+int redzone_occupancy(int w, int items, int block);
+int default_cfg(const rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
+int clamp_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
+
+// Hooks implemented by the tuning / learned-predictor translation units.
+bool predict_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, const uint32_t* d_idx,
+                 cudaStream_t s, rz_launch_cfg* cfg);
+bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
+void release_extras(rz_ctx* ctx);
+int read_status(rz_ctx* ctx, cudaStream_t s);
+
+// Test hook: run a grid barrier whose expected arrival count exceeds the grid, so that the
+// bounded wait must expire; returns the device status bits observed.
+int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out);
+
+}  // namespace rz

@@ -1,0 +1,218 @@
+"""GPU parity of the single-list Redzone kernels against the oracle, through the C-ABI."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import redzone_b200 as rz
+from redzone_b200 import workloads
+from tests import _golden, _torch_rule
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = rz.Context(0)
+    yield c
+    c.close()
+
+
+def payload(n, words, seed=0):
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, 1 << 32, size=(n, words), dtype=np.uint64).astype(np.uint32)
+    a[:, 0] = np.arange(n, dtype=np.uint32)
+    return a
+
+
+def run_gpu(ctx, host, idx, cfg=None, flags=rz.RZ_SYNC):
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    di = torch.from_numpy(idx.astype(np.int32)).to(DEV)
+    di_before = di.clone()
+    if cfg is None:
+        ctx.remove(d, di, flags=flags)
+    else:
+        ctx.remove_cfg(d, di, cfg, flags=flags)
+    torch.cuda.synchronize()
+    assert torch.equal(di, di_before), "the removal list must not be written"
+    return d.cpu().numpy().view(np.uint32)
+
+
+def expect_of(host, idx):
+    e = host.copy()
+    oracle.remove(e, idx)
+    return e
+
+
+def test_golden_vectors(ctx):
+    for case in _golden.cases():
+        n, k = case["n"], case["k"]
+        got = run_gpu(ctx, np.arange(n, dtype=np.uint32).reshape(n, 1), case["idx"])
+        assert _golden.check_prefix(case, got[: n - k, 0].view(np.int32)), case
+
+
+@pytest.mark.parametrize("words", [1, 2, 4, 8])
+@pytest.mark.parametrize("dist", ["uniform", "clustered", "tail", "red50", "red100", "red0"])
+def test_widths_and_distributions(ctx, words, dist):
+    for n, k in [(1 << 12, 1 << 8), (1 << 16, 1 << 12), (1 << 20, 1 << 16), (300000, 256 * 100)]:
+        if dist == "tail" and k > n // 10:
+            continue
+        if dist == "red0" and k > n // 2:
+            continue
+        host = payload(n, words, seed=n + k)
+        idx = workloads.make(dist, n, k, seed=k)
+        got = run_gpu(ctx, host, idx)
+        exp = expect_of(host, idx)
+        assert np.array_equal(got[: n - k], exp[: n - k]), (words, dist, n, k)
+        assert np.array_equal(got[n - k:], host[n - k:]), "tail must be left untouched"
+
+
+def test_every_launch_config_gives_the_same_bits(ctx):
+    """F1: the result depends only on (data, idx), never on block/items/grid."""
+    cases = [(1 << 20, 1 << 16, "uniform"), (1 << 18, 1 << 17, "red50"), (1 << 16, 3001, "red100")]
+    for n, k, dist in cases:
+        for words in (1, 4):
+            host = payload(n, words, seed=5)
+            idx = workloads.make(dist, n, k, seed=6)
+            exp = expect_of(host, idx)
+            for block in (128, 256, 512, 1024):
+                for items in (1, 2, 4, 8):
+                    for cps in (1, 2, 4):
+                        cfg = rz.LaunchCfg(block, items, cps, 0)
+                        got = run_gpu(ctx, host, idx, cfg=cfg)
+                        assert np.array_equal(got[: n - k], exp[: n - k]), (n, k, dist, words, block, items, cps)
+
+
+def test_single_cta_schedule(ctx):
+    for n, k in [(5000, 4000), (1 << 16, 1 << 14), (1 << 20, 1 << 17)]:
+        host = payload(n, 2, seed=1)
+        idx = workloads.uniform(n, k, seed=2)
+        got = run_gpu(ctx, host, idx, flags=rz.RZ_SYNC | rz.RZ_FORCE_BLOCK)
+        assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
+@pytest.mark.parametrize("n,k", [(1, 0), (1, 1), (2, 1), (7, 7), (100, 0), (100, 99), (100, 1), (33, 32), (4097, 4096)])
+def test_edge_sizes(ctx, n, k):
+    host = payload(n, 1, seed=n)
+    idx = workloads.uniform(n, k, seed=k)
+    got = run_gpu(ctx, host, idx)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
+def test_back_to_back_calls_leave_scratch_clean(ctx):
+    """Bitmap and barrier state are self-cleaning: many calls in a row stay exact."""
+    rng = np.random.default_rng(0)
+    for it in range(30):
+        n = int(rng.integers(1000, 1 << 20))
+        k = int(rng.integers(1, n))
+        host = payload(n, 1, seed=it)
+        idx = workloads.uniform(n, k, seed=it)
+        got = run_gpu(ctx, host, idx)
+        assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k]), it
+
+
+def test_validation_reports_and_leaves_data_untouched(ctx):
+    n, k = 1 << 16, 1000
+    host = payload(n, 1)
+    idx = workloads.uniform(n, k, seed=1)
+    dup = idx.copy()
+    dup[10] = dup[500]
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.remove(d, torch.from_numpy(dup.astype(np.int32)).to(DEV), flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+    assert e.value.code == 2
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), host)
+    bad = idx.copy()
+    bad[3] = n + 5
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.remove(d, torch.from_numpy(bad.astype(np.int32)).to(DEV), flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+    assert e.value.code == 3
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), host)
+    # A valid call right after the failures still gives the exact result.
+    got = run_gpu(ctx, host, idx, flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
+def test_out_of_range_without_validation_is_memory_safe(ctx):
+    """Bad indices never cause out-of-bounds accesses: an index >= n is ignored, reported."""
+    n, k = 1 << 14, 512
+    host = payload(n, 1)
+    idx = workloads.uniform(n, k, seed=3).astype(np.int64)
+    idx[7] = 0xFFFFFF00
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.remove(d, torch.from_numpy(idx.astype(np.uint32).view(np.int32)).to(DEV), flags=rz.RZ_SYNC)
+    assert e.value.code == 3
+
+
+def test_partition_matches_stable_oracle(ctx):
+    for words in (1, 2, 4, 8):
+        for n, k in [(1000, 10), (1 << 18, 1 << 12), (1 << 20, 1 << 19), (123457, 1)]:
+            host = payload(n, words, seed=words)
+            idx = workloads.uniform(n, k, seed=n)
+            d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+            ctx.partition(d, torch.from_numpy(idx.astype(np.int32)).to(DEV), flags=rz.RZ_SYNC)
+            exp = host.copy()
+            oracle.stable_remove(exp, idx)
+            got = d.cpu().numpy().view(np.uint32)
+            assert np.array_equal(got[: n - k], exp[: n - k]), (words, n, k)
+
+
+def test_bounded_barrier_wait_times_out_with_status(ctx):
+    bits = ctx.test_barrier_timeout(spin_limit=2000)
+    assert bits & 4
+    # The context is usable afterwards.
+    host = payload(1 << 16, 1)
+    idx = workloads.uniform(1 << 16, 1 << 12, seed=1)
+    got = run_gpu(ctx, host, idx)
+    assert np.array_equal(got[: (1 << 16) - (1 << 12)], expect_of(host, idx)[: (1 << 16) - (1 << 12)])
+
+
+def test_host_index_entry_point(ctx):
+    n, k = 1 << 20, 1 << 14
+    host = payload(n, 1)
+    idx = workloads.uniform(n, k, seed=8)
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    pinned = torch.from_numpy(idx.astype(np.int32)).pin_memory()
+    new_len = ctx.remove_host_idx(d, pinned)
+    assert new_len == n - k
+    got = d.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
+def test_reference_shaped_call():
+    n, k = 1 << 16, 1 << 10
+    a = torch.arange(n, dtype=torch.int32, device=DEV)
+    idx = workloads.uniform(n, k, seed=4)
+    r = torch.from_numpy(idx.astype(np.int32)).to(DEV)
+    new_len = rz.RemoveFromList(a, n, r, k, flags=rz.RZ_SYNC)
+    assert new_len == n - k
+    e = np.arange(n, dtype=np.int32)
+    oracle.remove(e, idx)
+    assert np.array_equal(a.cpu().numpy()[: n - k], e[: n - k])
+
+
+def test_torch_rule_matches_oracle():
+    n, k = 1 << 18, 1 << 15
+    host = payload(n, 1)
+    idx = workloads.red_split(n, k, seed=3, red_percentage=40)
+    t = _torch_rule.canonical_prefix(torch.from_numpy(host.view(np.int32)).to(DEV),
+                                     torch.from_numpy(idx.astype(np.int64)).to(DEV))
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), expect_of(host, idx)[: n - k])
+
+
+@pytest.mark.parametrize("k_log2,dist", [(16, "uniform"), (24, "tail"), (26, "uniform"), (27, "uniform"), (20, "clustered")])
+def test_full_size_n_2_28(ctx, k_log2, dist):
+    """n = 2^28 int32 iota (the large-list benchmark size): bit-exact against the torch
+    statement of the rule plus isOK_CPU's survivor properties."""
+    n, k = 1 << 28, 1 << k_log2
+    a = torch.arange(n, dtype=torch.int32, device=DEV)
+    idx = workloads.make_torch(dist, n, k, seed=k_log2)
+    exp = _torch_rule.canonical_prefix(a, idx)
+    ctx.remove(a, idx, flags=rz.RZ_SYNC)
+    assert torch.equal(a[: n - k], exp)
+    props = _torch_rule.survivor_properties(a[: n - k], n, idx)
+    assert all(props.values()), props
+    del a, exp
+    torch.cuda.empty_cache()

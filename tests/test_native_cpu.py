@@ -1,0 +1,57 @@
+"""Host-side checks of the native library that need no GPU: it loads, exports every function
+include/*.h declares, and its status strings are defined. No compute calls here."""
+import ctypes
+import subprocess
+
+import numpy as np
+
+from redzone_b200 import _native, workloads
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    names = _native.declared_symbols()
+    assert "rz_remove" in names and "rz_create" in names
+    missing = [nm for nm in names if not hasattr(_native.lib, nm)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_native.LIB_PATH)], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    assert set(names) <= exported
+
+
+def test_status_strings():
+    for code in range(9):
+        s = _native.status_string(code)
+        assert s and s != "unknown status"
+    assert _native.status_string(99) == "unknown status"
+
+
+def test_library_is_built_for_sm100a():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(_native.LIB_PATH)],
+                         capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_item_bytes():
+    import torch
+    from redzone_b200 import item_bytes
+    assert item_bytes(torch.zeros(10, dtype=torch.int32)) == 4
+    assert item_bytes(torch.zeros(10, 4, dtype=torch.int32)) == 16
+    assert item_bytes(torch.zeros(10, 4, dtype=torch.int64)) == 32
+
+
+def test_workload_distributions():
+    n = 1 << 16
+    u = workloads.uniform(n, 5000, 1)
+    assert u.dtype == np.uint32 and np.unique(u).size == 5000 and u.max() < n
+    c = workloads.clustered(n, 256 * 20, 2)
+    s = np.sort(c.astype(np.int64))
+    assert np.unique(s).size == s.size
+    starts = np.flatnonzero(np.diff(np.concatenate([[-10], s])) != 1)
+    runs = np.diff(np.concatenate([starts, [s.size]]))
+    assert (runs % 256 == 0).all()  # adjacent runs may touch, never overlap
+    t = workloads.tail(n, 3000, 3)
+    assert t.min() >= n - n // 10 and np.unique(t).size == 3000
+    r = workloads.red_split(n, 1000, 4, 25)
+    assert (r >= n - 1000).sum() == 250
+    nn, kk = workloads.batched_lists(4096, seed=0)
+    assert nn.min() >= 256 and nn.max() <= 1 << 22 and (kk <= nn // 2 + 1).all()
