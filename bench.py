@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of single-list Redzone removal on B200.
+
+Workload (the large-list configuration the headline target is quoted on): n = 2^28 int32 items
+(iota), k = 2^16 distinct removal indices drawn uniformly without replacement, unsorted. A step
+is one Redzone removal of k items from the device-resident list. L2 is flushed between timed
+steps (a 256 MiB scrub write), and the removal lists rotate over 8 seeds.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference] [--sweep]
+
+Own arm: CUDA-event time of each rz_remove kernel on the launching stream; value = k / mean
+step time (whole job: summed over ranks; N > 1 runs independent replicas, max over ranks).
+Also reported: roofline of the Redzone kernel against measured HBM bandwidth, the O(n)
+partition comparator on the same workload, an end-to-end figure through rz_remove_host_idx
+(removal list copied from pinned host memory, new length read back, every step), the
+reference's own CPU Redzone timed on this host, and SM clocks sampled during the timed region.
+
+Reference arm (--impl reference): the reference's redzone_CPU (compiled from its sources into
+oracle/_ref) on the same workload on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_LOG2, K_LOG2, W_BYTES = 28, 16, 4
+NSETS = 8
+SCRUB_BYTES = 256 << 20
+FALLBACK_HBM_GBS = 6650.0
+
+METRIC = "items removed/s"
+UNIT = "items/s"
+
+
+def config(parallelism: str) -> dict:
+    return {
+        "workload": f"single-list Redzone removal, n=2^{N_LOG2} int32 payload (iota), k=2^{K_LOG2} distinct "
+                    f"uniform unsorted indices",
+        "n": 1 << N_LOG2, "k": 1 << K_LOG2, "elem_bytes": W_BYTES, "distribution": "uniform",
+        "l2": "flushed between timed steps (256 MiB scrub write)", "index_sets": NSETS,
+        "parallelism": parallelism,
+    }
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def load_traffic(key: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get(key)
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def alg_bytes(n: int, k: int, w: int, idx: np.ndarray) -> float:
+    """Algorithmic bytes of one Redzone call: read R, read surviving tail items, write the holes,
+    write + read the k-bit red-zone bitmap: 4k + 2w(k - k_r) + k/4, k_r = #{R >= n-k}."""
+    k_r = int((idx >= n - k).sum())
+    return 4.0 * k + 2.0 * w * (k - k_r) + k / 4.0
+
+
+# ------------------------------------------------------------------------------------------------
+def cpu_reference_time(n: int, k: int, steps: int, warmup: int, time_budget_s: float):
+    """Time the reference's redzone_CPU (oracle/_ref) -- or the oracle port if it is absent."""
+    import oracle
+    from redzone_b200 import workloads
+
+    a = np.arange(n, dtype=np.int32)
+    sets = [workloads.uniform(n, k, seed=s).astype(np.int32) for s in range(NSETS)]
+    L = oracle.ref_lib()
+    if L is not None:
+        kind, cores = "reference", int(L.ref_redzone_threads())
+
+        def run(i):
+            r = sets[i % NSETS].copy()  # redzone_CPU clobbers its removal list
+            t0 = time.perf_counter()
+            L.ref_redzone_cpu(a.ctypes.data, n, r.ctypes.data, k)
+            return time.perf_counter() - t0
+    else:
+        kind, cores = "port", 1
+
+        def run(i):
+            r = sets[i % NSETS].astype(np.uint32)
+            t0 = time.perf_counter()
+            oracle.remove(a, r)
+            return time.perf_counter() - t0
+    for i in range(warmup):
+        run(i)
+    times = []
+    t_start = time.perf_counter()
+    for i in range(steps):
+        times.append(run(i))
+        if time.perf_counter() - t_start > time_budget_s and len(times) >= 3:
+            break
+    return kind, cores, times
+
+
+def reference_arm(args):
+    world, rank, _ = dist_init(args)
+    if rank != 0:
+        return
+    n, k = 1 << N_LOG2, 1 << K_LOG2
+    kind, cores, times = cpu_reference_time(n, k, args.steps, args.warmup, time_budget_s=120.0)
+    mean = statistics.mean(times)
+    v = k / mean
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "impl": "reference",
+        "config": config("host CPU, reference redzone_CPU"),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{len(times)} full calls of the workload (n=2^{N_LOG2}, k=2^{K_LOG2}); "
+                                   f"removal list restored before each call (the reference clobbers it)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------
+def own_arm(args):
+    import torch
+
+    world, rank, local = dist_init(args)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    import redzone_b200 as rz
+    from redzone_b200 import workloads
+    from tests import _torch_rule
+
+    ctx = rz.Context(dev.index)
+    n, k = 1 << N_LOG2, 1 << K_LOG2
+    a = torch.arange(n, dtype=torch.int32, device=dev)
+    sets_np = [workloads.uniform(n, k, seed=1000 * rank + s) for s in range(NSETS)]
+    sets = [torch.from_numpy(s.astype(np.int32)).to(dev) for s in sets_np]
+    pinned = [torch.from_numpy(s.astype(np.int32)).pin_memory() for s in sets_np]
+    scrub = torch.empty(SCRUB_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # Parity gate (not timed): the first call must equal the canonical result.
+    exp = _torch_rule.canonical_prefix(a, sets[0])
+    ctx.remove(a, sets[0], flags=rz.RZ_SYNC)
+    assert torch.equal(a[: n - k], exp), "parity check failed"
+    del exp
+    kernels_per_call, grid, block = ctx.last_launch()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- Redzone, device-resident inputs ----
+    for i in range(args.warmup):
+        ctx.remove(a, sets[i % NSETS])
+        scrub.fill_(i & 255)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(dev.index)
+    barrier()
+    clocks.start()
+    time.sleep(0.25)  # let the sampler attach before the timed region
+    region0 = torch.cuda.Event(enable_timing=True)
+    region1 = torch.cuda.Event(enable_timing=True)
+    region0.record(stream)
+    for i in range(args.steps):
+        starts[i].record(stream)
+        ctx.remove(a, sets[i % NSETS])
+        ends[i].record(stream)
+        scrub.fill_(i & 255)
+    region1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    mean_ms = max_over_ranks(statistics.mean(step_ms))
+    region_ms = max_over_ranks(region0.elapsed_time(region1))
+    value = world * k / (mean_ms * 1e-3)
+
+    # ---- O(n) partition comparator on the same workload (fewer steps; ~1 GiB read + write each) ----
+    p_steps = max(5, min(50, args.steps // 20))
+    p_ms = []
+    for i in range(p_steps + 2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.partition(a, sets[i % NSETS])
+        e1.record(stream)
+        scrub.fill_(i & 255)
+        if i >= 2:
+            p_ms.append((e0, e1))
+    torch.cuda.synchronize()
+    part_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in p_ms))
+
+    # ---- end to end through the public C-ABI with host buffers ----
+    e_steps = max(10, min(args.steps, 500))
+    e_ms = []
+    barrier()
+    for i in range(e_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        new_len = ctx.remove_host_idx(a, pinned[i % NSETS])
+        e1.record(stream)
+        assert new_len == n - k
+        e_ms.append((e0, e1))
+        scrub.fill_(i & 255)
+    barrier()
+    e2e_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in e_ms))
+
+    # ---- roofline of the Redzone kernel ----
+    balg = statistics.mean(alg_bytes(n, k, W_BYTES, s) for s in sets_np)
+    achieved = balg / (mean_ms * 1e-3) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic(f"redzone_single_n2e{N_LOG2}_k2e{K_LOG2}_w{W_BYTES}")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        kind, cores, times = cpu_reference_time(n, k, steps=50, warmup=2, time_budget_s=20.0)
+        cpu = {"value": k / statistics.mean(times), "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{len(times)} full calls of the same workload (n=2^{N_LOG2}, k=2^{K_LOG2}) on the host"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": config("single GPU" if world == 1 else f"{world} independent replicas (one list per GPU)"),
+            "timed_region_ms": region_ms,
+            "gpu_launches": args.steps * kernels_per_call,
+            "launch": {"grid": grid, "block": block, "kernels_per_call": kernels_per_call},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": balg, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6.65 TB/s"},
+            "partition_on": {"ms_per_step": part_ms, "speedup_redzone_vs_partition": part_ms / mean_ms},
+            "e2e": {"value": world * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 4 * k,
+                    "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------------
+def sweep(args):
+    """k sweep at n = 2^28 for int32 and 16-byte payloads, three distributions (one JSON per line)."""
+    import torch
+    import redzone_b200 as rz
+    from redzone_b200 import workloads
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    ctx = rz.Context(0)
+    n = 1 << N_LOG2
+    peak, _ = load_peaks()
+    scrub = torch.empty(SCRUB_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    ks = [int(x) for x in args.sweep_k.split(",")] if args.sweep_k else list(range(10, 28))
+    for w in (4, 16):
+        a = torch.zeros((n, w // 4), dtype=torch.int32, device=dev)
+        a[:, 0] = torch.arange(n, dtype=torch.int32, device=dev)
+        for dist in ("uniform", "clustered", "tail"):
+            for kl in ks:
+                k = 1 << kl
+                if dist == "tail" and k > n // 10:
+                    continue
+                idx = workloads.make_torch(dist, n, k, seed=kl).contiguous()
+                idx_np = idx.cpu().numpy().astype(np.int64)
+                reps = 20 if kl < 22 else 5
+                res = {}
+                for name, fn in (("redzone", lambda: ctx.remove(a, idx)), ("partition", lambda: ctx.partition(a, idx))):
+                    fn()
+                    ev = []
+                    for r in range(reps + (0 if name == "redzone" else 0)):
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        scrub.fill_(r & 255)
+                        e0.record(stream)
+                        fn()
+                        e1.record(stream)
+                        ev.append((e0, e1))
+                    torch.cuda.synchronize()
+                    res[name] = statistics.median(s.elapsed_time(e) for s, e in ev)
+                balg = alg_bytes(n, k, w, idx_np)
+                line = {"n": n, "k": k, "w": w, "dist": dist, "redzone_ms": res["redzone"],
+                        "partition_ms": res["partition"], "items_per_s": k / (res["redzone"] * 1e-3),
+                        "alg_bytes": balg, "achieved_gbs": balg / (res["redzone"] * 1e-3) / 1e9,
+                        "frac_of_hbm": balg / (res["redzone"] * 1e-3) / 1e9 / peak,
+                        "speedup_vs_partition": res["partition"] / res["redzone"]}
+                print(json.dumps(line), flush=True)
+                del idx
+        del a
+        torch.cuda.empty_cache()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["own", "reference"], default="own")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--sweep", action="store_true", help="run the k sweep instead of the headline")
+    ap.add_argument("--sweep-k", default="", help="comma-separated log2(k) values for --sweep")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    elif args.sweep:
+        sweep(args)
+    else:
+        own_arm(args)
+
+
+if __name__ == "__main__":
+    main()

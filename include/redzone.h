@@ -116,6 +116,10 @@ int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
                    rz_launch_cfg* cfg);
 
 /* ---- diagnostics -------------------------------------------------------------------------- */
+/* Number of kernels the context's most recent removal call launched (memsets not counted), and
+ * the grid / block it used for its main kernel. */
+int rz_last_launch(const rz_ctx* ctx, int32_t* kernels, int32_t* grid, int32_t* block);
+
 /*
  * Failure-detection check for the bounded device waits that replace the reference's grid
  * barriers (cg::grid.sync, redzone.hxx:707-940, and BlockStorage_t::Wait, redzone.hxx:59-80,

@@ -129,6 +129,12 @@ class Context:
         self._check(_native.lib.rz_default_cfg(self.handle, n, k, w, ctypes.byref(cfg)), "rz_default_cfg")
         return cfg
 
+    def last_launch(self) -> tuple[int, int, int]:
+        """(kernels launched, grid, block) of the most recent removal call on this context."""
+        a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _native.lib.rz_last_launch(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
     def test_barrier_timeout(self, spin_limit: int) -> int:
         bits = ctypes.c_uint32(0)
         self._check(_native.lib.rz_test_barrier_timeout(self.handle, spin_limit, ctypes.byref(bits)),

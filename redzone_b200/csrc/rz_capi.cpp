@@ -215,19 +215,27 @@ int rz_remove_cfg(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, con
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    ctx->last_kernels = 0;
+    ctx->last_grid = 0;
+    ctx->last_block = 0;
     if (k == 0 || k == n) {
         // Nothing moves (reference: redzone.hxx:651, Redzone_CPU.hxx handles it implicitly).
         if (flags & RZ_VALIDATE && k > 0) {
             st = launch_validate(ctx, uint32_t(n), d_idx, uint32_t(k), s);
             if (st != RZ_OK) return st;
+            ctx->last_kernels = 2;
         }
         return (flags & RZ_SYNC) ? read_status(ctx, s) : RZ_OK;
     }
+    LaunchInfo info;
     if (cfg->use_partition || (flags & RZ_FORCE_PARTITION))
-        st = launch_partition(ctx, d_data, uint32_t(n), elem_bytes, d_idx, uint32_t(k), flags, s, nullptr);
+        st = launch_partition(ctx, d_data, uint32_t(n), elem_bytes, d_idx, uint32_t(k), flags, s, &info);
     else
-        st = launch_redzone(ctx, d_data, uint32_t(n), elem_bytes, d_idx, uint32_t(k), *cfg, flags, s, nullptr);
+        st = launch_redzone(ctx, d_data, uint32_t(n), elem_bytes, d_idx, uint32_t(k), *cfg, flags, s, &info);
     if (st != RZ_OK) return st;
+    ctx->last_kernels = info.launches;
+    ctx->last_grid = info.grid;
+    ctx->last_block = info.block;
     return (flags & RZ_SYNC) ? read_status(ctx, s) : RZ_OK;
 }
 
@@ -287,6 +295,14 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
     st = read_status(ctx, s);
     if (new_len) *new_len = (k > 0 && k < n) ? int64_t(dl) : n - k;
     return st;
+}
+
+int rz_last_launch(const rz_ctx* ctx, int32_t* kernels, int32_t* grid, int32_t* block) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    if (kernels) *kernels = ctx->last_kernels;
+    if (grid) *grid = ctx->last_grid;
+    if (block) *block = ctx->last_block;
+    return RZ_OK;
 }
 
 int rz_test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_bits) {

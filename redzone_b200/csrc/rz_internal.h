@@ -55,6 +55,9 @@ struct rz_ctx {
     rz::Workspace ws;
     std::string last_cuda_error;
     std::recursive_mutex mu;
+    int last_kernels = 0;        // kernels launched by the most recent removal call
+    int last_grid = 0;
+    int last_block = 0;
     void* predictor = nullptr;   // rz::Predictor*, owned (see rz_mlp.cu)
     void* tune_table = nullptr;  // rz::TuneTable*, owned (see rz_autotune.cpp)
 };
