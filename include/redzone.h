@@ -58,12 +58,21 @@ typedef enum rz_status {
 #define RZ_USE_PREDICTOR   0x20u /* let the trained MLP pick the launch configuration            */
 #define RZ_ALLOW_STABLE    0x40u /* caller accepts the partition path's (stable) survivor order  */
 
-/* Launch configuration of the single-list kernels (one entry of the 48-point tuning space). */
+/* Schedules of the single-list Redzone kernel. */
+#define RZ_SCHED_AUTO    0  /* cluster for small/medium k, grid-wide otherwise                    */
+#define RZ_SCHED_BLOCK   1  /* one CTA, block-level synchronisation                              */
+#define RZ_SCHED_CLUSTER 2  /* one thread-block cluster; red-zone bitmap in distributed smem      */
+#define RZ_SCHED_GRID    3  /* persistent grid, bounded global barriers                           */
+
+/* Launch configuration of the single-list kernels (one entry of the 48-point tuning space:
+ * block x items x grid scale, plus the Redzone-vs-partition bit). */
 typedef struct rz_launch_cfg {
     int32_t block;          /* threads per CTA: 128, 256, 512 or 1024                             */
     int32_t items;          /* items per thread per tile: 1, 2, 4 or 8                            */
-    int32_t ctas_per_sm;    /* grid = ctas_per_sm x SM count (capped by occupancy and tile count) */
+    int32_t ctas_per_sm;    /* grid scale g in {1,2,4}: grid schedule = g CTAs per SM (capped by  */
+                            /* occupancy and tile count); cluster schedule = 4g CTAs per cluster */
     int32_t use_partition;  /* 1 = O(n) partition path, 0 = Redzone                                */
+    int32_t schedule;       /* RZ_SCHED_*                                                          */
 } rz_launch_cfg;
 
 /* ---- context ------------------------------------------------------------------------------ */
@@ -119,6 +128,16 @@ int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
 /* Number of kernels the context's most recent removal call launched (memsets not counted), and
  * the grid / block it used for its main kernel. */
 int rz_last_launch(const rz_ctx* ctx, int32_t* kernels, int32_t* grid, int32_t* block);
+
+/*
+ * Phase tracing of the single-list Redzone kernels (the reference's clock64 phase stamps,
+ * redzone.hxx:629,708-712,847-851,936-939, kept per CTA and in %globaltimer nanoseconds).
+ * When enabled, thread 0 of every CTA records 8 slots: 0 start, 1 marks issued, 2 first barrier
+ * passed, 3 holes filled / orphans listed, 4 done; 5-7 unused. rz_read_phase_stamps synchronises
+ * the device and copies the stamps of the most recent call (8 * nctas values).
+ */
+int rz_phase_stamps(rz_ctx* ctx, int enable);
+int rz_read_phase_stamps(rz_ctx* ctx, uint64_t* out, int32_t max_ctas, int32_t* nctas);
 
 /*
  * Failure-detection check for the bounded device waits that replace the reference's grid

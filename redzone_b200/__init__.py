@@ -135,6 +135,18 @@ class Context:
         _native.lib.rz_last_launch(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
         return a.value, b.value, c.value
 
+    def phase_stamps(self, enable: bool) -> None:
+        """Turn per-CTA %globaltimer phase stamps of the Redzone kernels on or off."""
+        self._check(_native.lib.rz_phase_stamps(self.handle, 1 if enable else 0), "rz_phase_stamps")
+
+    def read_phase_stamps(self):
+        """Stamps of the most recent call as a (ctas, 8) uint64 numpy array (ns)."""
+        import numpy as np
+        buf = (ctypes.c_uint64 * (1024 * 8))()
+        n = ctypes.c_int32(0)
+        self._check(_native.lib.rz_read_phase_stamps(self.handle, buf, 1024, ctypes.byref(n)), "rz_read_phase_stamps")
+        return np.ctypeslib.as_array(buf)[: n.value * 8].reshape(n.value, 8).copy()
+
     def test_barrier_timeout(self, spin_limit: int) -> int:
         bits = ctypes.c_uint32(0)
         self._check(_native.lib.rz_test_barrier_timeout(self.handle, spin_limit, ctypes.byref(bits)),

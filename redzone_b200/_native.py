@@ -23,14 +23,19 @@ c_vp, c_i32, c_u32, c_i64, c_u64, c_f32 = (ctypes.c_void_p, ctypes.c_int32, ctyp
                                            ctypes.c_int64, ctypes.c_uint64, ctypes.c_float)
 
 
+RZ_SCHED_AUTO, RZ_SCHED_BLOCK, RZ_SCHED_CLUSTER, RZ_SCHED_GRID = 0, 1, 2, 3
+
+
 class LaunchCfg(ctypes.Structure):
-    _fields_ = [("block", c_i32), ("items", c_i32), ("ctas_per_sm", c_i32), ("use_partition", c_i32)]
+    _fields_ = [("block", c_i32), ("items", c_i32), ("ctas_per_sm", c_i32), ("use_partition", c_i32),
+                ("schedule", c_i32)]
 
     def as_tuple(self):
-        return (self.block, self.items, self.ctas_per_sm, self.use_partition)
+        return (self.block, self.items, self.ctas_per_sm, self.use_partition, self.schedule)
 
     def __repr__(self):
-        return f"LaunchCfg(block={self.block}, items={self.items}, ctas_per_sm={self.ctas_per_sm}, partition={self.use_partition})"
+        return (f"LaunchCfg(block={self.block}, items={self.items}, ctas_per_sm={self.ctas_per_sm}, "
+                f"partition={self.use_partition}, schedule={self.schedule})")
 
 
 # Status codes (rz_status).
@@ -67,6 +72,8 @@ _sig("rz_partition", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINT
 _sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchCfg)])
 _sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
 _sig("rz_last_launch", c_i32, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)])
+_sig("rz_phase_stamps", c_i32, [c_vp, c_i32])
+_sig("rz_read_phase_stamps", c_i32, [c_vp, ctypes.POINTER(c_u64), c_i32, ctypes.POINTER(c_i32)])
 
 
 def status_string(code: int) -> str:

@@ -58,7 +58,8 @@ int ensure_seen(rz_ctx* ctx, size_t n) {
 int ensure_partition(rz_ctx* ctx, size_t n, size_t ntiles) {
     int st = grow(ctx, ctx->ws.part_bits, ctx->ws.part_words, (n + 31) / 32 + 1, true);
     if (st != RZ_OK) return st;
-    return grow(ctx, ctx->ws.tile_state, ctx->ws.tile_cap, ntiles + 1, true);
+    // Ticket line (16 words) + three 32-bit arrays of ntiles (staged, kept, offset).
+    return grow(ctx, ctx->ws.tile_state, ctx->ws.tile_cap, 16 + (3 * ntiles + 1) / 2 + 1, true);
 }
 
 int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {
@@ -67,7 +68,9 @@ int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {
     if (w.bitmap) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.bitmap, 0, w.bitmap_words * 4, s));
     if (w.seen) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.seen, 0, w.seen_words * 4, s));
     if (w.part_bits) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.part_bits, 0, w.part_words * 4, s));
-    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.sync, 0, sizeof(GridSync), s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.epoch, 0, 4, s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.arrive, 0, kMaxGrid * 4, s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.cnt_words, 0, 2 * kMaxGrid * 8, s));
     w.dirty = false;
     return RZ_OK;
 }
@@ -132,8 +135,12 @@ int rz_create(rz_ctx** out, int device) {
     ctx->smem_optin = prop.sharedMemPerBlockOptin;
     Workspace& w = ctx->ws;
     void* p = nullptr;
-    // status | GridSync | counts | dev_len, one allocation.
-    const size_t bytes = 256 + sizeof(GridSync) + 2 * kMaxGrid * 4 + 256;
+    // One allocation: status | epoch | dev_len (one 256-byte line each) | arrival tags |
+    // tagged orphan counts | phase stamps.
+    const size_t off_arrive = 768;
+    const size_t off_cnt = off_arrive + size_t(kMaxGrid) * 4;
+    const size_t off_stamps = off_cnt + size_t(2 * kMaxGrid) * 8;
+    const size_t bytes = off_stamps + size_t(kMaxGrid) * kStampsPerCta * 8;
     e = cudaMalloc(&p, bytes);
     if (e == cudaSuccess) e = cudaMemset(p, 0, bytes);
     if (e != cudaSuccess) {
@@ -143,9 +150,11 @@ int rz_create(rz_ctx** out, int device) {
     }
     uint8_t* b = static_cast<uint8_t*>(p);
     w.status = reinterpret_cast<uint32_t*>(b);
-    w.sync = reinterpret_cast<GridSync*>(b + 256);
-    w.counts = reinterpret_cast<uint32_t*>(b + 256 + sizeof(GridSync));
-    w.dev_len = reinterpret_cast<unsigned long long*>(b + 256 + sizeof(GridSync) + 2 * kMaxGrid * 4);
+    w.epoch = reinterpret_cast<uint32_t*>(b + 256);
+    w.dev_len = reinterpret_cast<unsigned long long*>(b + 512);
+    w.arrive = reinterpret_cast<uint32_t*>(b + off_arrive);
+    w.cnt_words = reinterpret_cast<unsigned long long*>(b + off_cnt);
+    w.stamps = reinterpret_cast<unsigned long long*>(b + off_stamps);
     *out = ctx;
     return RZ_OK;
 }
@@ -302,6 +311,25 @@ int rz_last_launch(const rz_ctx* ctx, int32_t* kernels, int32_t* grid, int32_t* 
     if (kernels) *kernels = ctx->last_kernels;
     if (grid) *grid = ctx->last_grid;
     if (block) *block = ctx->last_block;
+    return RZ_OK;
+}
+
+int rz_phase_stamps(rz_ctx* ctx, int enable) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    ctx->ws.stamps_on = enable != 0;
+    return RZ_OK;
+}
+
+int rz_read_phase_stamps(rz_ctx* ctx, uint64_t* out, int32_t max_ctas, int32_t* nctas) {
+    if (!ctx || !out || max_ctas < 0) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    const int n = std::min<int>(max_ctas, std::min(ctx->last_grid, kMaxGrid));
+    RZ_CUDA_TRY(ctx, cudaDeviceSynchronize());
+    if (n > 0)
+        RZ_CUDA_TRY(ctx, cudaMemcpy(out, ctx->ws.stamps, size_t(n) * kStampsPerCta * 8, cudaMemcpyDeviceToHost));
+    if (nctas) *nctas = n;
     return RZ_OK;
 }
 

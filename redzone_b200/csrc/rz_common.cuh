@@ -1,8 +1,8 @@
 // rz_common.cuh -- device-side building blocks shared by every Redzone kernel in this library.
 //
 // Contents: payload types for the four supported element widths, acquire/release memory
-// operations in inline PTX, a self-resetting generation barrier with a bounded wait (the
-// replacement for cg::this_grid().sync() and BlockStorage_t::Wait(), redzone.hxx:56-80 and
+// operations in inline PTX, epoch-tagged arrival flags with bounded waits (the replacement for
+// cg::this_grid().sync() and BlockStorage_t::Wait(), redzone.hxx:56-80 and
 // :707,846,912,935,940), and a few warp/block scan helpers.
 #pragma once
 
@@ -60,42 +60,117 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-// ---- generation barrier -----------------------------------------------------------------------
-// {count, gen} live in library scratch. Each participating CTA reads `gen`, then arrives on
-// `count`; the last arriver resets `count` and publishes gen+1 with release semantics. Because
-// the last arriver always leaves count at zero, the pair needs no per-call reset and is safe
-// under CUDA-graph replay. A CTA that passes `wait=false` arrives without waiting (used when it
-// has no work after the barrier). Every wait is bounded by `spin_limit` polls; on expiry the CTA
-// records ST_TIMEOUT and the function returns false, so no kernel ever hangs.
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, uint32_t expected, bool wait,
-                                             uint32_t* status, uint32_t spin_limit) {
-    __shared__ int s_ok;
+// ---- epoch-tagged arrival flags --------------------------------------------------------------
+// The grid schedule's barriers. Each call reads an epoch E once at kernel start and tags every
+// arrival with E+1; a CTA arrives with one release store to its own slot and waits by polling the
+// other CTAs' slots for the tag. Flags from earlier calls carry older tags, so nothing is reset
+// between calls (graph replays included). CTA 0 advances the stored epoch once every CTA has
+// arrived at the first barrier, i.e. after every CTA of this call has read it.
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Record a phase timestamp for this CTA when tracing is enabled (params carry `stamps`).
+#define RZ_STAMP(p, slot)                                                                          \
+    do {                                                                                           \
+        if ((p).stamps && threadIdx.x == 0)                                                        \
+            (p).stamps[blockIdx.x * ::rz::kStampsPerCta + (slot)] = ::rz::globaltimer();           \
+    } while (0)
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Arrive: the barrier orders every thread's prior writes before thread 0's release store.
+__device__ __forceinline__ void flag_arrive(uint32_t* flags, uint32_t slot, uint32_t tag) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const uint32_t g0 = ld_acquire(&gs->gen);
-        const uint32_t old = atom_add_acq_rel(&gs->count, 1u);
-        if (old == expected - 1) {
-            atomicExch(&gs->count, 0u);
-            __threadfence();
-            st_release(&gs->gen, g0 + 1u);
-        } else if (wait) {
-            uint32_t it = 0;
-            uint32_t ns = 32;
-            while (ld_acquire(&gs->gen) == g0) {
-                if (++it > spin_limit) {
-                    ok = 0;
-                    atomicOr(status, ST_TIMEOUT);
-                    break;
-                }
-                __nanosleep(ns);
-                if (ns < 256) ns <<= 1;
+    if (threadIdx.x == 0) st_release(&flags[slot], tag);
+}
+
+// Wait until flags[0..G) all hold `tag`; bounded by spin_limit polls per slot. The polls are
+// relaxed and back-to-back (each is an L2 round trip; __nanosleep backoff was measured to add
+// microseconds of wake-up latency per barrier on B200); one acquire fence by thread 0, ordered
+// before the rest of the block by the closing barrier, makes the other CTAs' released writes
+// visible. Returns false (and records ST_TIMEOUT) if some slot never gets there.
+__device__ __forceinline__ bool flag_wait_all(const uint32_t* flags, uint32_t G, uint32_t tag, uint32_t* status,
+                                              uint32_t spin_limit) {
+    int ok = 1;
+    for (uint32_t c = threadIdx.x; c < G && ok; c += blockDim.x) {
+        uint32_t it = 0;
+        while (ld_relaxed(&flags[c]) != tag) {
+            if (++it > spin_limit) {
+                ok = 0;
+                break;
             }
         }
-        s_ok = ok;
     }
+    const int all = __syncthreads_and(ok);
+    if (!all) {
+        if (threadIdx.x == 0) atomicOr(status, ST_TIMEOUT);
+        return false;
+    }
+    if (threadIdx.x == 0) fence_acq_rel_gpu();
     __syncthreads();
-    return s_ok != 0;
+    return true;
+}
+
+// Prefetch the 128-byte lines that start inside [p, p + bytes) into L2, spread over the block's
+// threads (every prefetched address lies inside the range; the first partial line is left to the
+// demand load). A prefetch is not a memory access a fence waits for, so issuing it before a
+// barrier costs nothing there.
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+    const uintptr_t b = reinterpret_cast<uintptr_t>(p);
+    const uintptr_t lo = (b + 127) & ~uintptr_t(127);
+    const uintptr_t hi = b + bytes;
+    for (uintptr_t a = lo + uintptr_t(threadIdx.x) * 128; a < hi; a += uintptr_t(blockDim.x) * 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+}
+
+// ---- mbarrier + 1-D TMA bulk copies (no multicast) ---------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Arrive once and add `bytes` to the transaction count the current phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Global -> shared bulk copy completing on `bar`. Both addresses 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void tma_load_1d(void* dst_smem, const void* src, uint32_t bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst_smem)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 // ---- scans ------------------------------------------------------------------------------------

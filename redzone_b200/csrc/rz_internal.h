@@ -12,14 +12,8 @@
 
 namespace rz {
 
-// Generation-barrier state (see grid_barrier in rz_common.cuh): one 128-byte line.
-struct GridSync {
-    uint32_t count;
-    uint32_t gen;
-    uint32_t pad[30];
-};
-
 constexpr int kMaxGrid = 1024;           // upper bound on CTAs of the persistent single-list kernel
+constexpr int kStampsPerCta = 8;         // phase timestamps recorded per CTA when enabled
 constexpr uint32_t kSpinLimit = 1u << 22;  // polls of a bounded device wait (~0.5-1 s with backoff)
 
 // Library scratch owned by one context. Every buffer is zero where the kernels require it on
@@ -27,8 +21,6 @@ constexpr uint32_t kSpinLimit = 1u << 22;  // polls of a bounded device wait (~0
 // needed; `dirty` forces a full re-zero after a call that ended with a device error.
 struct Workspace {
     uint32_t* status = nullptr;      // device status word (ST_* bits)
-    GridSync* sync = nullptr;        // generation barrier state
-    uint32_t* counts = nullptr;      // 2 * kMaxGrid per-CTA orphan counts
     uint32_t* bitmap = nullptr;      // red-zone bitmap, k bits
     size_t bitmap_words = 0;
     uint32_t* dlist = nullptr;       // destination orphans (per-CTA regions), k entries
@@ -38,11 +30,16 @@ struct Workspace {
     size_t seen_words = 0;
     uint32_t* part_bits = nullptr;   // partition path: n-bit removal map
     size_t part_words = 0;
-    unsigned long long* tile_state = nullptr;  // partition path: look-back state + ticket
+    unsigned long long* tile_state = nullptr;  // partition path: ticket, staged/kept/offset per tile
     size_t tile_cap = 0;
     unsigned long long* dev_len = nullptr;     // device copy of the last new length
     uint32_t* idx_stage = nullptr;   // rz_remove_host_idx: device copy of host indices
     size_t stage_cap = 0;
+    uint32_t* epoch = nullptr;       // grid schedule: call epoch (advanced by CTA 0 each call)
+    uint32_t* arrive = nullptr;      // grid schedule: per-CTA arrival tags, kMaxGrid
+    unsigned long long* cnt_words = nullptr;  // grid schedule: tagged orphan counts, 2*kMaxGrid
+    unsigned long long* stamps = nullptr;     // optional phase timestamps, 8 per CTA
+    bool stamps_on = false;
     bool dirty = false;
 };
 
@@ -90,6 +87,12 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
                    LaunchInfo* info);
 int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx,
                      uint32_t k, uint32_t flags, cudaStream_t s, LaunchInfo* info);
+// Cluster schedule (rz_cluster.cu); RZ_ERR_UNSUPPORTED when the bitmap slice does not fit in
+// shared memory or no cluster of the requested size can be co-scheduled.
+int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
+                   const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
+int cluster_max_block(int w, int items);
+constexpr uint32_t kClusterMaxK = 1u << 20;  // RZ_SCHED_AUTO uses the cluster schedule up to here
 int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cudaStream_t s);
 // Largest block size the single-list kernel for (w, items) can launch with.
 int redzone_max_block(int w, int items);

@@ -1,4 +1,4 @@
-// rz_single.cu -- single-list Redzone (persistent, grid-wide) and the O(n) partition comparator.
+// rz_single.cu -- single-list Redzone, persistent grid-wide schedule (and the single-CTA case).
 //
 // Redzone follows Algorithm 2 of the reference (RemoveFromList_GPUWide, redzone.hxx:626-941) and
 // its CPU form (redzone_CPU, Redzone_CPU.hxx:150-248). The phases are the reference's; the data
@@ -6,18 +6,19 @@
 //   * Phase A (mark, reference :698-706): every index in the red zone [cut, n) sets one bit of a
 //     k-bit bitmap in scratch (atomicOr) instead of writing an in-band 0x80000000 sentinel into
 //     the caller's tail, so any payload width works and the tail is never written.
-//   * Grid barrier: a bounded generation barrier (rz_common.cuh) replaces cg::grid.sync().
+//   * Barrier: epoch-tagged arrival flags with bounded waits (rz_common.cuh) replace
+//     cg::grid.sync() and BlockStorage_t::Wait(): one release store per CTA, no reset.
 //   * Phase B (fill holes, reference :752-822): items are processed in tiles of B*IPT, item
 //     (j, t) of a tile at i = base + j*B + t, so every warp load of the index list and of the tail
 //     window is a contiguous 128-byte (or 32*W-byte) segment. Valid/valid pairs are moved at once;
 //     orphans get their rank in i order from per-(j, warp) ballot counts and one scan per tile,
 //     and are written to per-CTA regions of scratch lists (the caller's index list is const).
 //     Each tile clears the bitmap words it read, which leaves the bitmap zero for the next call.
-//   * Phase C (pair orphans, reference :834-934): only CTAs that own destination orphans wait for
-//     the others; they prefix the per-CTA counts and binary-search the owner of each source rank
-//     (instead of the reference's LoadBalance linear search, :477-524).
-// The partition comparator is a mark pass plus a single-pass, in-place, stable compaction with
-// decoupled look-back (the O(n) algorithms of cuCompactor.cuh:29-87 and Thrust_remove.hxx:15-17).
+//   * Phase C (pair orphans, reference :834-934): each CTA publishes its two orphan counts as
+//     epoch-tagged words; only CTAs that own destination orphans wait for the others, prefix the
+//     counts and binary-search the owner of each source rank (instead of the reference's
+//     LoadBalance linear search, :477-524).
+// The O(n) partition comparator is in rz_partition.cu; the cluster schedule in rz_cluster.cu.
 #include <algorithm>
 #include <cstdio>
 
@@ -33,10 +34,12 @@ struct SingleParams {
     uint32_t* bitmap;
     uint32_t* dlist;
     uint32_t* slist;
-    uint32_t* counts;
-    GridSync* sync;
+    uint32_t* epoch;
+    uint32_t* arrive;
+    unsigned long long* cnt_words;
     uint32_t* status;
     unsigned long long* dev_len;
+    unsigned long long* stamps;  // nullable: 8 globaltimer stamps per CTA
     uint32_t spin_limit;
     uint32_t validate;
 };
@@ -47,6 +50,7 @@ struct SingleParams {
 template <int W, int IPT>
 __global__ void redzone_single_kernel(const SingleParams p) {
     using T = typename Payload<W>::T;
+    RZ_STAMP(p, 0);
     T* __restrict__ head = reinterpret_cast<T*>(p.data);
     const uint32_t n = p.n, k = p.k, cut = n - k;
     const T* __restrict__ tail = reinterpret_cast<const T*>(p.data) + cut;
@@ -65,12 +69,11 @@ __global__ void redzone_single_kernel(const SingleParams p) {
     __shared__ uint32_t s_pd[kMaxGrid + 1];
     __shared__ uint32_t s_ps[kMaxGrid + 1];
     __shared__ int s_abort;
+    __shared__ uint32_t s_tag;
 
-    if (p.validate) {
-        // Validation ran earlier in the stream; on failure leave the caller's data untouched.
-        if (threadIdx.x == 0) s_abort = (__ldcg(p.status) & (ST_DUPLICATE | ST_RANGE)) != 0;
-        __syncthreads();
-        if (s_abort) return;
+    if (threadIdx.x == 0) {
+        s_tag = (G > 1) ? ld_acquire(p.epoch) + 1u : 0u;
+        s_abort = p.validate ? ((__ldcg(p.status) & (ST_DUPLICATE | ST_RANGE)) != 0) : 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && p.dev_len) *p.dev_len = (unsigned long long)(n - k);
 
@@ -78,6 +81,7 @@ __global__ void redzone_single_kernel(const SingleParams p) {
     T src[IPT];
 
     // ---- phase A: mark the red zone ---------------------------------------------------------
+    // The loads are issued before the first __syncthreads so they overlap the epoch read.
     for (uint32_t t = t0; t < t1; ++t) {
         const uint32_t base = t * TILE;
 #pragma unroll
@@ -86,12 +90,14 @@ __global__ void redzone_single_kernel(const SingleParams p) {
             rr[j] = (i < k) ? __ldg(&p.idx[i]) : 0xffffffffu;
         }
         if (single) {
-            // Issue the tail loads now; they complete while the grid waits at the barrier.
-#pragma unroll
-            for (int j = 0; j < IPT; ++j) {
-                const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-                if (i < k) src[j] = tail[i];
-            }
+            // Pull this CTA's tail window into L2 while the grid waits at the barrier. A prefetch
+            // is not an outstanding access the arrival's release has to wait for (a load is).
+            const uint32_t cnt = min(TILE, k - base);
+            prefetch_l2(tail + base, size_t(cnt) * W);
+        }
+        if (t == t0) {
+            __syncthreads();  // s_abort / s_tag
+            if (s_abort) return;  // validation failed: leave the caller's data untouched
         }
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
@@ -103,22 +109,40 @@ __global__ void redzone_single_kernel(const SingleParams p) {
                 } else {
                     const uint32_t off = r - cut;
                     const uint32_t bit = 1u << (off & 31u);
-                    const uint32_t old = atomicOr(&p.bitmap[off >> 5], bit);
-                    if (p.validate && (old & bit)) atomicOr(p.status, ST_DUPLICATE);
+                    if (p.validate) {
+                        if (atomicOr(&p.bitmap[off >> 5], bit) & bit) atomicOr(p.status, ST_DUPLICATE);
+                    } else {
+                        atomicOr(&p.bitmap[off >> 5], bit);
+                    }
                 }
             }
         }
     }
+    if (t0 >= t1) {
+        __syncthreads();
+        if (s_abort) return;
+    }
+    RZ_STAMP(p, 1);
+    const uint32_t tag = s_tag;
     if (G > 1) {
-        if (!grid_barrier(p.sync, G, true, p.status, p.spin_limit)) return;
+        flag_arrive(p.arrive, blockIdx.x, tag);
+        RZ_STAMP(p, 5);
+        if (!flag_wait_all(p.arrive, G, tag, p.status, p.spin_limit)) return;
+        // Every CTA has read the epoch (it arrived): advance it for the next call.
+        if (blockIdx.x == 0 && threadIdx.x == 0) *p.epoch = tag;
     } else {
-        __threadfence_block();
         __syncthreads();
     }
+    RZ_STAMP(p, 2);
 
     // ---- phase B: classify, fill holes, collect orphans --------------------------------------
+    // With one tile per CTA the hole writes are issued only after the orphan counts have been
+    // published (below), so the publishing release does not wait for ~k scattered stores.
     uint32_t dcnt = 0, scnt = 0;
     const int E = IPT * nw;
+    bool dv[IPT], sv[IPT];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) dv[j] = sv[j] = false;
     for (uint32_t t = t0, tt = 0; t < t1; ++t, ++tt) {
         const uint32_t base = t * TILE;
         if (!single) {
@@ -128,12 +152,12 @@ __global__ void redzone_single_kernel(const SingleParams p) {
                 rr[j] = (i < k) ? __ldg(&p.idx[i]) : 0xffffffffu;
             }
         }
-        bool dv[IPT], sv[IPT];
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
             if (i < k) {
                 const uint32_t word = __ldcg(&p.bitmap[i >> 5]);
+                if (single) src[j] = tail[i];  // L2 hit (prefetched), issued with the bitmap load
                 sv[j] = ((word >> (i & 31u)) & 1u) == 0u;
                 dv[j] = rr[j] < cut;
             } else {
@@ -147,10 +171,10 @@ __global__ void redzone_single_kernel(const SingleParams p) {
                 const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
                 if (dv[j] && sv[j]) src[j] = tail[i];
             }
-        }
 #pragma unroll
-        for (int j = 0; j < IPT; ++j)
-            if (dv[j] && sv[j]) head[rr[j]] = src[j];
+            for (int j = 0; j < IPT; ++j)
+                if (dv[j] && sv[j]) head[rr[j]] = src[j];
+        }
 
         uint32_t dmask[IPT], smask[IPT];
         uint32_t* cbuf = s_cnt[tt & 1u];
@@ -204,25 +228,54 @@ __global__ void redzone_single_kernel(const SingleParams p) {
         dcnt += tot >> 16;
         scnt += tot & 0xffffu;
     }
+    RZ_STAMP(p, 3);
 
     // ---- phase C: pair destination orphans with source orphans of equal global rank ------------
     if (G > 1) {
+        __syncthreads();  // this CTA's orphan-list writes precede the release below
         if (threadIdx.x == 0) {
-            p.counts[blockIdx.x] = dcnt;
-            p.counts[G + blockIdx.x] = scnt;
-            __threadfence();
+            const unsigned long long hi = (unsigned long long)tag << 32;
+            st_release_u64(&p.cnt_words[blockIdx.x], hi | dcnt);
+            st_release_u64(&p.cnt_words[G + blockIdx.x], hi | scnt);
         }
-        if (!grid_barrier(p.sync, G, dcnt > 0u, p.status, p.spin_limit)) return;
-        if (dcnt == 0u) return;
-        for (uint32_t c = threadIdx.x; c < G; c += B) {
-            s_pd[c] = __ldcg(&p.counts[c]);
-            s_ps[c] = __ldcg(&p.counts[G + c]);
+    }
+    if (single) {
+#pragma unroll
+        for (int j = 0; j < IPT; ++j)
+            if (dv[j] && sv[j]) head[rr[j]] = src[j];
+    }
+    if (G > 1) {
+        if (dcnt == 0u) {
+            RZ_STAMP(p, 4);
+            return;
         }
+        int ok = 1;
+        for (uint32_t c = threadIdx.x; c < 2 * G && ok; c += B) {
+            uint32_t it = 0;
+            unsigned long long w = ld_relaxed_u64(&p.cnt_words[c]);
+            while (uint32_t(w >> 32) != tag) {
+                if (++it > p.spin_limit) {
+                    ok = 0;
+                    break;
+                }
+                w = ld_relaxed_u64(&p.cnt_words[c]);
+            }
+            if (c < G) s_pd[c] = uint32_t(w);
+            else s_ps[c - G] = uint32_t(w);
+        }
+        if (!__syncthreads_and(ok)) {
+            if (threadIdx.x == 0) atomicOr(p.status, ST_TIMEOUT);
+            return;
+        }
+        if (threadIdx.x == 0) fence_acq_rel_gpu();  // the other CTAs' source-orphan lists
         __syncthreads();
         block_scan_array(s_pd, int(G), s_scan);
         block_scan_array(s_ps, int(G), s_scan);
     } else {
-        if (dcnt == 0u) return;
+        if (dcnt == 0u) {
+            RZ_STAMP(p, 4);
+            return;
+        }
         if (threadIdx.x == 0) {
             s_pd[0] = 0; s_pd[1] = dcnt;
             s_ps[0] = 0; s_ps[1] = scnt;
@@ -243,6 +296,7 @@ __global__ void redzone_single_kernel(const SingleParams p) {
         const uint32_t dest = __ldcg(&p.dlist[chunk_base + r]);
         head[dest] = reinterpret_cast<const T*>(p.data)[pos];
     }
+    RZ_STAMP(p, 4);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -269,154 +323,12 @@ __global__ void validate_clear_kernel(const uint32_t* __restrict__ idx, uint32_t
 }
 
 // ------------------------------------------------------------------------------------------------
-// O(n) partition comparator: mark, then stable in-place compaction with decoupled look-back.
+// Barrier-timeout test kernel: the grid's own arrival protocol, waiting for one CTA more than the
+// grid has, so the bounded wait must expire.
 // ------------------------------------------------------------------------------------------------
-__global__ void partition_mark_kernel(const uint32_t* __restrict__ idx, uint32_t k, uint32_t n,
-                                      uint32_t* __restrict__ bits, uint32_t* status, uint32_t validate) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
-        const uint32_t r = __ldg(&idx[i]);
-        if (r >= n) {
-            atomicOr(status, ST_RANGE);
-            continue;
-        }
-        const uint32_t bit = 1u << (r & 31u);
-        const uint32_t old = atomicOr(&bits[r >> 5], bit);
-        if (validate && (old & bit)) atomicOr(status, ST_DUPLICATE);
-    }
-}
-
-// Look-back state word: bits 62-63 = flag (1 aggregate, 2 inclusive prefix), bits 0-61 = value.
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagInc = 2ull << 62;
-constexpr unsigned long long kValMask = (1ull << 62) - 1;
-
-template <int W, int IPT>
-__global__ void partition_compact_kernel(uint8_t* data, uint32_t n, uint32_t* __restrict__ bits,
-                                         unsigned long long* state, uint32_t* status,
-                                         uint32_t spin_limit, unsigned long long* dev_len,
-                                         uint32_t new_len) {
-    using T = typename Payload<W>::T;
-    T* A = reinterpret_cast<T*>(data);
-    const int B = blockDim.x, nw = B >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t TILE = uint32_t(B) * IPT;
-    unsigned long long* ticket = state;       // state[0] = ticket counter
-    unsigned long long* tstate = state + 1;   // per-tile look-back words
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_cnt[8 * 32 + 1];
-    __shared__ unsigned long long s_excl;
-    // The tile's values pass through shared memory: the store needs each load's result, so once
-    // the barrier below completes every load of this tile has landed. Only then may the tile
-    // publish its count, which lets later tiles write over this tile's input range.
-    __shared__ T s_stage[IPT * 256];
-    if (threadIdx.x == 0) s_tile = uint32_t(atomicAdd(ticket, 1ull));
-    if (blockIdx.x == 0 && threadIdx.x == 0 && dev_len) *dev_len = new_len;
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint32_t base = tile * TILE;
-
-    T v[IPT];
-    bool keep[IPT];
-    if (B > 256) return;  // s_stage is sized for 256 threads (the only block size launched)
-#pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-        const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-        keep[j] = false;
-        if (i < n) {
-            v[j] = A[i];
-            const uint32_t word = __ldcg(&bits[i >> 5]);
-            keep[j] = ((word >> (i & 31u)) & 1u) == 0u;
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < IPT; ++j)
-        if (base + uint32_t(j) * B + threadIdx.x < n) s_stage[j * B + threadIdx.x] = v[j];
-    uint32_t km[IPT];
-#pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-        km[j] = __ballot_sync(0xffffffffu, keep[j]);
-        if (lane == 0) s_cnt[j * nw + warp] = __popc(km[j]);
-    }
-    if (lane == 0) {
-#pragma unroll
-        for (int j = 0; j < IPT; ++j) {
-            const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-            if (i < n) bits[i >> 5] = 0u;
-        }
-    }
-    __syncthreads();
-    const int E = IPT * nw;
-    if (warp == 0) {
-        const int per = (E + 31) >> 5;
-        const int lo = lane * per, hi = min(lo + per, E);
-        uint32_t s = 0;
-        for (int e = lo; e < hi; ++e) s += s_cnt[e];
-        const uint32_t inc = warp_inclusive_scan(s);
-        uint32_t run = inc - s;
-        for (int e = lo; e < hi; ++e) {
-            const uint32_t x = s_cnt[e];
-            s_cnt[e] = run;
-            run += x;
-        }
-        if (lane == 31) s_cnt[E] = inc;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        const unsigned long long agg = s_cnt[E];
-        if (lane == 0) {
-            __threadfence();
-            st_release_u64(&tstate[tile], (tile == 0 ? kFlagInc : kFlagAgg) | agg);
-        }
-        unsigned long long excl = 0;
-        if (tile > 0) {
-            int64_t pred = int64_t(tile) - 1 - lane;
-            bool done = false;
-            uint32_t it = 0;
-            while (!done) {
-                unsigned long long s = kFlagInc;  // lanes before tile 0 act as a zero prefix
-                if (pred >= 0) {
-                    s = ld_acquire_u64(&tstate[pred]);
-                    while ((s >> 62) == 0ull) {
-                        if (++it > spin_limit) break;
-                        __nanosleep(32);
-                        s = ld_acquire_u64(&tstate[pred]);
-                    }
-                }
-                if (__any_sync(0xffffffffu, it > spin_limit)) {
-                    if (lane == 0) atomicOr(status, ST_TIMEOUT);
-                    excl = 0;
-                    break;
-                }
-                const uint32_t incmask = __ballot_sync(0xffffffffu, (s >> 62) == 2ull);
-                // Lanes up to and including the nearest inclusive prefix contribute.
-                const int stop = incmask ? __ffs(incmask) - 1 : 32;
-                unsigned long long val = (lane <= stop) ? (pred >= 0 ? (s & kValMask) : 0ull) : 0ull;
-#pragma unroll
-                for (int d = 16; d > 0; d >>= 1) val += __shfl_down_sync(0xffffffffu, val, d);
-                excl += __shfl_sync(0xffffffffu, val, 0);
-                if (incmask) done = true;
-                else pred -= 32;
-            }
-            if (lane == 0) st_release_u64(&tstate[tile], kFlagInc | (excl + agg));
-        }
-        if (lane == 0) s_excl = excl;
-    }
-    __syncthreads();
-    const unsigned long long excl = s_excl;
-    const uint32_t lt = lanemask_lt();
-#pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-        if (keep[j]) {
-            const unsigned long long dst = excl + s_cnt[j * nw + warp] + __popc(km[j] & lt);
-            A[dst] = s_stage[j * B + threadIdx.x];
-        }
-    }
-}
-
-// ------------------------------------------------------------------------------------------------
-// Barrier-timeout test kernel: one CTA waits for an arrival count that can never be reached.
-// ------------------------------------------------------------------------------------------------
-__global__ void barrier_timeout_kernel(GridSync* gs, uint32_t* status, uint32_t spin_limit) {
-    grid_barrier(gs, gridDim.x + 1u, true, status, spin_limit);
+__global__ void barrier_timeout_kernel(uint32_t* arrive, uint32_t* status, uint32_t spin_limit, uint32_t tag) {
+    flag_arrive(arrive, blockIdx.x, tag);
+    flag_wait_all(arrive, gridDim.x + 1u, tag, status, spin_limit);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -483,14 +395,14 @@ int clamp_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg) {
 int default_cfg(const rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg) {
     (void)n;
     cfg->use_partition = 0;
-    if (k <= 2048u) {
-        cfg->block = 256; cfg->items = 8; cfg->ctas_per_sm = 1;
-    } else if (k <= (1u << 22)) {
-        cfg->block = 256; cfg->items = 4; cfg->ctas_per_sm = 1;
+    cfg->schedule = RZ_SCHED_AUTO;
+    if (k <= kClusterMaxK) {
+        // One 16-CTA cluster; up to 2^16 items this is a single tile per CTA.
+        cfg->block = 1024; cfg->items = 4; cfg->ctas_per_sm = 4;
     } else {
         cfg->block = 512; cfg->items = 4; cfg->ctas_per_sm = 2;
     }
-    if (w >= 16 && cfg->items > 4) cfg->items = 4;
+    if (w >= 16 && cfg->items > 2) cfg->items = 2;
     return clamp_cfg(ctx, k, w, cfg);
 }
 
@@ -520,15 +432,29 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
         if (st != RZ_OK) return st;
         launches += 2;
     }
+    int sched = cfg.schedule;
+    if (flags & RZ_FORCE_BLOCK) sched = RZ_SCHED_BLOCK;
+    if (flags & RZ_FORCE_GRID) sched = RZ_SCHED_GRID;
+    if (sched == RZ_SCHED_AUTO) sched = (k <= kClusterMaxK) ? RZ_SCHED_CLUSTER : RZ_SCHED_GRID;
+    if (sched == RZ_SCHED_CLUSTER) {
+        LaunchInfo ci;
+        ci.launches = launches;
+        st = launch_cluster(ctx, data, n, w, idx, k, cfg, validate, s, &ci);
+        if (st == RZ_OK) {
+            if (info) *info = ci;
+            return RZ_OK;
+        }
+        if (st != RZ_ERR_UNSUPPORTED) return st;
+        sched = RZ_SCHED_GRID;  // bitmap slice too large for shared memory: use the grid schedule
+    }
     const uint32_t tile = uint32_t(cfg.block) * uint32_t(cfg.items);
     const uint32_t ntiles = (k + tile - 1) / tile;
     int occ = redzone_occupancy(int(w), cfg.items, cfg.block);
     if (occ <= 0) return RZ_ERR_INVALID_ARG;
     long grid = std::min<long>((long)cfg.ctas_per_sm, (long)occ) * ctx->sms;
-    if (cfg.ctas_per_sm <= 0) grid = ctx->sms;
     grid = std::min<long>(grid, (long)ntiles);
     grid = std::min<long>(grid, (long)kMaxGrid);
-    if (flags & RZ_FORCE_BLOCK) grid = 1;
+    if (sched == RZ_SCHED_BLOCK) grid = 1;
     if (grid < 1) grid = 1;
     // Re-balance: use as many CTAs as needed for the resulting tiles-per-CTA (no idle CTAs).
     const uint32_t tpc = (ntiles + uint32_t(grid) - 1) / uint32_t(grid);
@@ -542,10 +468,12 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     p.bitmap = ctx->ws.bitmap;
     p.dlist = ctx->ws.dlist;
     p.slist = ctx->ws.slist;
-    p.counts = ctx->ws.counts;
-    p.sync = ctx->ws.sync;
+    p.epoch = ctx->ws.epoch;
+    p.arrive = ctx->ws.arrive;
+    p.cnt_words = ctx->ws.cnt_words;
     p.status = ctx->ws.status;
     p.dev_len = ctx->ws.dev_len;
+    p.stamps = ctx->ws.stamps_on ? ctx->ws.stamps : nullptr;
     p.spin_limit = kSpinLimit;
     p.validate = validate ? 1u : 0u;
 
@@ -571,53 +499,18 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     return RZ_OK;
 }
 
-template <int W>
-static void (*part_fn())(uint8_t*, uint32_t, uint32_t*, unsigned long long*, uint32_t*, uint32_t,
-                         unsigned long long*, uint32_t) {
-    constexpr int IPT = W == 4 ? 8 : W == 8 ? 8 : W == 16 ? 4 : 2;
-    return partition_compact_kernel<W, IPT>;
-}
-static int part_items(int w) { return w == 4 ? 8 : w == 8 ? 8 : w == 16 ? 4 : 2; }
-
-int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
-                     uint32_t flags, cudaStream_t s, LaunchInfo* info) {
-    const int block = 256;
-    const int items = part_items(int(w));
-    const uint32_t tile = uint32_t(block * items);
-    const uint32_t ntiles = (n + tile - 1) / tile;
-    int st = ensure_partition(ctx, n, ntiles);
-    if (st != RZ_OK) return st;
-    st = reset_if_dirty(ctx, s);
-    if (st != RZ_OK) return st;
-    const bool validate = (flags & RZ_VALIDATE) != 0;
-    RZ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->ws.tile_state, 0, sizeof(unsigned long long) * (size_t(ntiles) + 1), s));
-    const int mgrid = std::max(1, std::min<int>(ctx->sms * 8, int((k + 255) / 256)));
-    partition_mark_kernel<<<mgrid, 256, 0, s>>>(idx, k, n, ctx->ws.part_bits, ctx->ws.status, validate ? 1u : 0u);
-    auto* f = w == 4 ? part_fn<4>() : w == 8 ? part_fn<8>() : w == 16 ? part_fn<16>() : part_fn<32>();
-    f<<<ntiles, block, 0, s>>>(static_cast<uint8_t*>(data), n, ctx->ws.part_bits, ctx->ws.tile_state,
-                               ctx->ws.status, kSpinLimit, ctx->ws.dev_len, n - k);
-    RZ_CUDA_TRY(ctx, cudaGetLastError());
-    if (info) {
-        info->grid = int(ntiles);
-        info->block = block;
-        info->items = items;
-        info->launches = 2;  // the look-back state memset is a copy-engine node, not a kernel
-    }
-    return RZ_OK;
-}
-
 int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out) {
     cudaStream_t s = nullptr;
     int st = reset_if_dirty(ctx, s);
     if (st != RZ_OK) return st;
-    barrier_timeout_kernel<<<1, 32, 0, s>>>(ctx->ws.sync, ctx->ws.status, spin_limit);
+    // A tag no real call uses; the slots it leaves behind are reset below.
+    barrier_timeout_kernel<<<1, 32, 0, s>>>(ctx->ws.arrive, ctx->ws.status, spin_limit, 0xfffffff0u);
     RZ_CUDA_TRY(ctx, cudaGetLastError());
     RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
     uint32_t h = 0;
     RZ_CUDA_TRY(ctx, cudaMemcpy(&h, ctx->ws.status, sizeof(h), cudaMemcpyDeviceToHost));
     RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
-    // The abandoned arrival left the barrier counter at 1: reset the barrier state.
-    RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.sync, 0, sizeof(GridSync)));
+    ctx->ws.dirty = true;  // re-zero the barrier state before the next call
     *status_out = h;
     return RZ_OK;
 }

@@ -68,8 +68,12 @@ def test_widths_and_distributions(ctx, words, dist):
         assert np.array_equal(got[n - k:], host[n - k:]), "tail must be left untouched"
 
 
-def test_every_launch_config_gives_the_same_bits(ctx):
-    """F1: the result depends only on (data, idx), never on block/items/grid."""
+SCHEDULES = {"cluster": 2, "grid": 3}
+
+
+@pytest.mark.parametrize("sched", ["cluster", "grid"])
+def test_every_launch_config_gives_the_same_bits(ctx, sched):
+    """The result depends only on (data, idx), never on schedule, block, items or grid."""
     cases = [(1 << 20, 1 << 16, "uniform"), (1 << 18, 1 << 17, "red50"), (1 << 16, 3001, "red100")]
     for n, k, dist in cases:
         for words in (1, 4):
@@ -79,9 +83,20 @@ def test_every_launch_config_gives_the_same_bits(ctx):
             for block in (128, 256, 512, 1024):
                 for items in (1, 2, 4, 8):
                     for cps in (1, 2, 4):
-                        cfg = rz.LaunchCfg(block, items, cps, 0)
+                        cfg = rz.LaunchCfg(block, items, cps, 0, SCHEDULES[sched])
                         got = run_gpu(ctx, host, idx, cfg=cfg)
-                        assert np.array_equal(got[: n - k], exp[: n - k]), (n, k, dist, words, block, items, cps)
+                        assert np.array_equal(got[: n - k], exp[: n - k]), (sched, n, k, dist, words, block, items, cps)
+
+
+@pytest.mark.parametrize("sched", ["cluster", "grid"])
+@pytest.mark.parametrize("words", [1, 2, 4, 8])
+def test_schedules_on_large_k(ctx, sched, words):
+    n = 1 << 21
+    for k in (1 << 18, 1 << 20, (1 << 20) + 12345):
+        host = payload(n, words, seed=k)
+        idx = workloads.uniform(n, k, seed=k)
+        got = run_gpu(ctx, host, idx, cfg=rz.LaunchCfg(256, 4, 4, 0, SCHEDULES[sched]))
+        assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k]), (sched, words, k)
 
 
 def test_single_cta_schedule(ctx):
