@@ -120,6 +120,20 @@ int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
                  const uint32_t* d_idx, int64_t k, int64_t* new_len, uint32_t flags,
                  rz_stream_t stream);
 
+/*
+ * rz_remove for callers that cannot allocate device memory (an exhausted or foreign-owned memory
+ * pool, a real-time path that must not take the allocator's lock or synchronise, a plugin host
+ * that owns every allocation). No counterpart in the reference: its GPU path takes a
+ * caller-allocated BlockStorage_t instead. Needs no context and calls no allocating routine; its
+ * scratch is a fixed device-global array of about 8.4 MB that every GPU loading this library
+ * holds until exit. Limits: k <= 2^20 (RZ_ERR_UNSUPPORTED above that), n < 2^32. The first call
+ * on a device, with that device current, looks up the array's address: make it before any stream
+ * capture. Calls share the array, so calls that overlap on the GPU race; order them on one
+ * stream. Asynchronous on `stream`; same result as rz_remove; no RZ_VALIDATE.
+ */
+int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
+                      int64_t* new_len, rz_stream_t stream);
+
 /* The configuration rz_remove would choose for (n, k, elem_bytes) without a predictor. */
 int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
                    rz_launch_cfg* cfg);
