@@ -138,6 +138,70 @@ int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, const uint32
 int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
                    rz_launch_cfg* cfg);
 
+/* ---- many lists in one launch --------------------------------------------------------------- */
+/* One list: device pointers to its payload (n items) and its k distinct removal indices. */
+typedef struct rz_list_desc {
+    void* data;
+    const uint32_t* idx;
+    int64_t n;
+    int64_t k;
+} rz_list_desc;
+
+/* Tile and schedule of the batched kernel: tile = block * items; lists with k <= tile run whole
+ * in one CTA, longer lists are split into tiles and handed out `span` tiles per work item
+ * (0 = automatic: up to 8, at least ~32 items per list); ctas_per_sm sets the persistent grid. */
+typedef struct rz_batch_cfg {
+    int32_t block;
+    int32_t items;
+    int32_t ctas_per_sm;
+    int32_t span;
+} rz_batch_cfg;
+
+typedef struct rz_batch_plan rz_batch_plan;
+
+/*
+ * Plan the removal of every list of `lists` (host array) in one persistent launch. The plan owns
+ * its work queue and scratch. cfg == NULL uses the context's tuned batched configuration.
+ * Each list's result equals rz_remove on that list (the reference's per-list calls,
+ * redzone.hxx:1089-1166, one launch each).
+ */
+int  rz_batch_plan_create(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
+                          const rz_batch_cfg* cfg, rz_batch_plan** plan);
+/* Run the plan on `stream`: captured into a CUDA graph on the first launch, replayed after. */
+int  rz_batch_plan_launch(rz_batch_plan* plan, rz_stream_t stream);
+int  rz_batch_plan_info(const rz_batch_plan* plan, int32_t* grid, int32_t* block, int32_t* items,
+                        int64_t* work_items, int64_t* total_k);
+void rz_batch_plan_destroy(rz_batch_plan* plan);
+/* One-shot form: plan, run, synchronise, return the device status. */
+int  rz_remove_batched(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
+                       uint32_t flags, rz_stream_t stream);
+
+/* ---- autotuning ------------------------------------------------------------------------------ */
+typedef struct rz_tune_entry {
+    rz_launch_cfg cfg;
+    float ms;               /* median time of the configuration */
+} rz_tune_entry;
+
+/*
+ * Time the 48 launch configurations (block x items x grid scale, schedule chosen by k) and the
+ * partition path on the caller's data, which every run rewrites (timing does not depend on the
+ * values). L2 is flushed between repetitions. Writes up to max_out entries sorted by time.
+ */
+int rz_autotune_single(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx,
+                       int64_t k, int32_t reps, rz_tune_entry* out, int32_t max_out, int32_t* count);
+/* Time candidate batched configurations on `lists`; *best receives the fastest. */
+int rz_autotune_batched(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
+                        int32_t reps, rz_batch_cfg* best, float* best_ms);
+/*
+ * Tuning tables (text; '#' comments; lines "single <w> <log2k> <block> <items> <g> <partition>"
+ * and "batched <w> <block> <items> <ctas_per_sm>"). rz_remove and rz_batch_plan_create use the
+ * loaded entries (nearest log2 k bucket of the same width).
+ */
+int rz_tune_table_load(rz_ctx* ctx, const char* path);
+int rz_tune_table_save(rz_ctx* ctx, const char* path);
+int rz_tune_table_set_single(rz_ctx* ctx, uint32_t elem_bytes, int32_t log2k, const rz_launch_cfg* cfg);
+int rz_tune_table_set_batched(rz_ctx* ctx, uint32_t elem_bytes, const rz_batch_cfg* cfg);
+
 /* ---- diagnostics -------------------------------------------------------------------------- */
 /* Number of kernels the context's most recent removal call launched (memsets not counted), and
  * the grid / block it used for its main kernel. */

@@ -154,6 +154,65 @@ class Context:
         return bits.value
 
 
+def list_descs(lists) -> "ctypes.Array":
+    """[(data_tensor, idx_tensor), ...] -> rz_list_desc array (tensors must stay alive)."""
+    arr = (_native.ListDesc * len(lists))()
+    for q, (d, i) in enumerate(lists):
+        arr[q].data = d.data_ptr() if d.numel() else None
+        arr[q].idx = i.data_ptr() if i.numel() else None
+        arr[q].n = int(d.shape[0])
+        arr[q].k = int(i.numel())
+    return arr
+
+
+class BatchPlan:
+    """Many lists removed by one persistent launch, replayed from a CUDA graph (rz_batch_plan_*).
+
+    ``lists`` is a sequence of (data, idx) tensor pairs of the same item width; the tensors must
+    stay alive (and in place) as long as the plan is used.
+    """
+
+    def __init__(self, ctx: Context, lists, cfg: "_native.BatchCfg | None" = None):
+        self.ctx = ctx
+        self._descs = list_descs(lists)
+        w = item_bytes(lists[0][0]) if lists else 4
+        h = ctypes.c_void_p()
+        st = _native.lib.rz_batch_plan_create(ctx.handle, self._descs, len(lists), w,
+                                              ctypes.byref(cfg) if cfg is not None else None, ctypes.byref(h))
+        ctx._check(st, "rz_batch_plan_create")
+        self.handle = h
+
+    def launch(self, stream=None) -> None:
+        self.ctx._check(_native.lib.rz_batch_plan_launch(self.handle, ctypes.c_void_p(_stream_handle(stream))),
+                        "rz_batch_plan_launch")
+
+    def info(self) -> dict:
+        g, b, i = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        wi, tk = ctypes.c_int64(), ctypes.c_int64()
+        _native.lib.rz_batch_plan_info(self.handle, ctypes.byref(g), ctypes.byref(b), ctypes.byref(i),
+                                       ctypes.byref(wi), ctypes.byref(tk))
+        return {"grid": g.value, "block": b.value, "items": i.value, "work_items": wi.value, "total_k": tk.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _native.lib.rz_batch_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def remove_batched(ctx: Context, lists, stream=None) -> None:
+    """One-shot batched removal (plan, run, synchronise)."""
+    descs = list_descs(lists)
+    w = item_bytes(lists[0][0]) if lists else 4
+    ctx._check(_native.lib.rz_remove_batched(ctx.handle, descs, len(lists), w, 0,
+                                             ctypes.c_void_p(_stream_handle(stream))), "rz_remove_batched")
+
+
 _default: dict[int, Context] = {}
 
 

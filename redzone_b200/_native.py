@@ -52,6 +52,21 @@ RZ_USE_PREDICTOR = 0x20
 RZ_ALLOW_STABLE = 0x40
 
 
+class ListDesc(ctypes.Structure):
+    _fields_ = [("data", c_vp), ("idx", c_vp), ("n", c_i64), ("k", c_i64)]
+
+
+class BatchCfg(ctypes.Structure):
+    _fields_ = [("block", c_i32), ("items", c_i32), ("ctas_per_sm", c_i32), ("span", c_i32)]
+
+    def __repr__(self):
+        return f"BatchCfg(block={self.block}, items={self.items}, ctas_per_sm={self.ctas_per_sm})"
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("cfg", LaunchCfg), ("ms", c_f32)]
+
+
 def _sig(name, restype, argtypes):
     f = getattr(lib, name)
     f.restype = restype
@@ -73,6 +88,21 @@ _sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchC
 _sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
 _sig("rz_last_launch", c_i32, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)])
 _sig("rz_remove_noalloc", c_i32, [c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_vp])
+_sig("rz_batch_plan_create", c_i32, [c_vp, ctypes.POINTER(ListDesc), c_i32, c_u32, ctypes.POINTER(BatchCfg),
+                                     ctypes.POINTER(c_vp)])
+_sig("rz_batch_plan_launch", c_i32, [c_vp, c_vp])
+_sig("rz_batch_plan_info", c_i32, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32),
+                                   ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)])
+_sig("rz_batch_plan_destroy", None, [c_vp])
+_sig("rz_remove_batched", c_i32, [c_vp, ctypes.POINTER(ListDesc), c_i32, c_u32, c_u32, c_vp])
+_sig("rz_autotune_single", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, c_i32, ctypes.POINTER(TuneEntry), c_i32,
+                                   ctypes.POINTER(c_i32)])
+_sig("rz_autotune_batched", c_i32, [c_vp, ctypes.POINTER(ListDesc), c_i32, c_u32, c_i32, ctypes.POINTER(BatchCfg),
+                                    ctypes.POINTER(c_f32)])
+_sig("rz_tune_table_load", c_i32, [c_vp, ctypes.c_char_p])
+_sig("rz_tune_table_save", c_i32, [c_vp, ctypes.c_char_p])
+_sig("rz_tune_table_set_single", c_i32, [c_vp, c_u32, c_i32, ctypes.POINTER(LaunchCfg)])
+_sig("rz_tune_table_set_batched", c_i32, [c_vp, c_u32, ctypes.POINTER(BatchCfg)])
 _sig("rz_phase_stamps", c_i32, [c_vp, c_i32])
 _sig("rz_read_phase_stamps", c_i32, [c_vp, ctypes.POINTER(c_u64), c_i32, ctypes.POINTER(c_i32)])
 

@@ -1,13 +1,14 @@
-// rz_extras.cpp -- configuration hooks used by rz_remove before the tuning table and the learned
-// predictor are loaded into a context.
+// rz_extras.cpp -- context teardown of the optional parts (tuning table, learned predictor).
 #include "rz_internal.h"
 
 namespace rz {
 
-bool predict_cfg(rz_ctx*, uint32_t, uint32_t, uint32_t, const uint32_t*, cudaStream_t, rz_launch_cfg*) {
-    return false;
+void release_tune(rz_ctx* ctx);       // rz_autotune.cpp
+void release_predictor(rz_ctx* ctx);  // rz_mlp.cu
+
+void release_extras(rz_ctx* ctx) {
+    release_tune(ctx);
+    release_predictor(ctx);
 }
-bool tuned_cfg(rz_ctx*, uint32_t, uint32_t, uint32_t, rz_launch_cfg*) { return false; }
-void release_extras(rz_ctx*) {}
 
 }  // namespace rz

@@ -92,7 +92,9 @@ int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint
 int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                    const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int cluster_max_block(int w, int items);
-constexpr uint32_t kClusterMaxK = 1u << 20;  // RZ_SCHED_AUTO uses the cluster schedule up to here
+constexpr uint32_t kClusterMaxK = 1u << 14;  // RZ_SCHED_AUTO uses the cluster schedule up to here
+// The 48-point launch-configuration space in its canonical order (rz_autotune.cpp).
+void config_space(rz_launch_cfg* out48);
 int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cudaStream_t s);
 // Largest block size the single-list kernel for (w, items) can launch with.
 int redzone_max_block(int w, int items);
