@@ -176,6 +176,56 @@ void rz_batch_plan_destroy(rz_batch_plan* plan);
 int  rz_remove_batched(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
                        uint32_t flags, rz_stream_t stream);
 
+/* ---- streaming delete service ---------------------------------------------------------------- */
+/*
+ * A device-resident table split into `shards` independent sub-tables of shard_capacity records;
+ * delete batches (one shard, distinct live row indices) are submitted from the host while earlier
+ * ones run. A worker thread admits a batch when its shard has nothing in flight, a slot (stream)
+ * is free and its indices fit the slot's share of index_budget_bytes; it coalesces the admitted
+ * batches of a slot into one batched Redzone launch; slots overlap on the GPU. Live lengths are
+ * tracked on the device. Before a batch would take a shard below floor_rows the shard is refilled
+ * to capacity with fresh records (add-then-remove). No counterpart in the reference, which only
+ * benchmarks one removal at a time (tests.cu:135-157).
+ */
+typedef struct rz_service rz_service;
+
+typedef struct rz_service_cfg {
+    int32_t shards;
+    int32_t slots;                   /* launches in flight at once, one stream each               */
+    int64_t shard_capacity;          /* records per shard (< 2^32)                                  */
+    uint32_t record_bytes;           /* 4, 8, 16 or 32                                              */
+    int32_t max_batches_per_launch;  /* coalescing limit (distinct shards per launch)               */
+    int64_t index_budget_bytes;      /* device memory for in-flight indices, split over the slots */
+    int64_t floor_rows;              /* refill threshold                                            */
+} rz_service_cfg;
+
+typedef struct rz_service_stats {
+    int64_t submitted, completed, rejected, rows_deleted, launches, refills, rows_appended;
+    double p50_us, p99_us, mean_us, max_us;  /* per-batch latency, submit -> completion         */
+    double mean_batches_per_launch;
+    double busy_seconds;                     /* first submit -> last completion                */
+} rz_service_stats;
+
+#define RZ_SUBMIT_BORROW 0x1u  /* h_idx stays valid and unchanged until the batch completes */
+
+int  rz_service_create(rz_ctx* ctx, void* d_table, const int64_t* initial_len, const rz_service_cfg* cfg,
+                       rz_service** svc);
+/* RZ_ERR_BUSY: the batch is larger than one slot's index memory and can never be admitted. */
+int  rz_service_submit(rz_service* svc, int32_t shard, const uint32_t* h_idx, int64_t count,
+                       uint32_t flags, uint64_t* ticket);
+int  rz_service_drain(rz_service* svc, int32_t timeout_ms);
+int  rz_service_stats_get(rz_service* svc, rz_service_stats* out);
+int  rz_service_reset_stats(rz_service* svc);
+/* Live lengths as the host plans them and as the device tracks them (either pointer may be NULL). */
+int  rz_service_lengths(rz_service* svc, int64_t* host_view, int64_t* device_view);
+void rz_service_destroy(rz_service* svc);
+/* Load generator: Poisson arrivals at `rate` batches/s for `seconds`; each arrival submits a random
+ * batch of `pool` (pinned index arrays, lent to the service) to a uniformly random shard; then
+ * drains and returns the statistics. */
+int  rz_service_run_poisson(rz_service* svc, const uint32_t* const* pool, const int64_t* pool_counts,
+                            int32_t pool_size, double rate, double seconds, uint64_t seed,
+                            rz_service_stats* out);
+
 /* ---- autotuning ------------------------------------------------------------------------------ */
 typedef struct rz_tune_entry {
     rz_launch_cfg cfg;
@@ -201,6 +251,39 @@ int rz_tune_table_load(rz_ctx* ctx, const char* path);
 int rz_tune_table_save(rz_ctx* ctx, const char* path);
 int rz_tune_table_set_single(rz_ctx* ctx, uint32_t elem_bytes, int32_t log2k, const rz_launch_cfg* cfg);
 int rz_tune_table_set_batched(rz_ctx* ctx, uint32_t elem_bytes, const rz_batch_cfg* cfg);
+
+/* ---- learned configuration predictor ---------------------------------------------------------- */
+/*
+ * A 12 -> 64 -> 64 -> 49 FP32 MLP (ReLU hidden layers) trained and evaluated by the library's
+ * own CUDA kernels. Outputs 0..47 are logits over the 48 launch configurations (the order of
+ * rz_autotune_single's space), output 48 the logit of "the O(n) partition path is faster". The
+ * reference has no counterpart: its configuration is fixed at compile time (tests.cu:1-2).
+ * Features (rz_mlp_features, computed on the GPU from the index list): log2 n, log2 k, k/n,
+ * payload bytes, mean and variance of the log-gap of the sorted 4096-index sample, fraction of
+ * the sample in the red zone, 5-bucket run-length histogram (each scaled to about [0, 1]).
+ */
+typedef struct rz_mlp rz_mlp;
+int  rz_mlp_param_count(void);
+int  rz_mlp_create(rz_ctx* ctx, uint64_t seed, rz_mlp** mlp);
+void rz_mlp_destroy(rz_mlp* mlp);
+int  rz_mlp_get_params(rz_mlp* mlp, float* h_params, int32_t count);
+int  rz_mlp_set_params(rz_mlp* mlp, const float* h_params, int32_t count);
+int  rz_mlp_features(rz_ctx* ctx, const uint32_t* d_idx, int64_t n, int64_t k, uint32_t elem_bytes,
+                     float* h_features12);
+/* Logits (nsamp x 49) for host features (nsamp x 12). */
+int  rz_mlp_forward(rz_mlp* mlp, const float* h_x, int64_t nsamp, float* h_out);
+/* Mean loss and gradient of every parameter over one batch; targets nsamp x 49 (48 probabilities
+ * over configurations + the partition bit). Used to check the kernels against a CPU oracle. */
+int  rz_mlp_gradients(rz_mlp* mlp, const float* h_x, const float* h_t, int64_t nsamp, float* h_grad,
+                      float* h_loss);
+/* Adam on the GPU over nsamp samples, `epochs` passes of seeded mini-batches. */
+int  rz_mlp_train(rz_mlp* mlp, const float* h_x, const float* h_t, int64_t nsamp, int32_t epochs,
+                  int32_t batch, float lr, uint64_t seed, float* h_last_loss);
+/* Make rz_remove(..., RZ_USE_PREDICTOR) consult `mlp` (NULL detaches it). */
+int  rz_set_predictor(rz_ctx* ctx, rz_mlp* mlp);
+/* The configuration the attached predictor picks for an instance. */
+int  rz_predict_cfg(rz_ctx* ctx, const uint32_t* d_idx, int64_t n, int64_t k, uint32_t elem_bytes,
+                    rz_launch_cfg* cfg);
 
 /* ---- diagnostics -------------------------------------------------------------------------- */
 /* Number of kernels the context's most recent removal call launched (memsets not counted), and

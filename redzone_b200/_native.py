@@ -103,6 +103,46 @@ _sig("rz_tune_table_load", c_i32, [c_vp, ctypes.c_char_p])
 _sig("rz_tune_table_save", c_i32, [c_vp, ctypes.c_char_p])
 _sig("rz_tune_table_set_single", c_i32, [c_vp, c_u32, c_i32, ctypes.POINTER(LaunchCfg)])
 _sig("rz_tune_table_set_batched", c_i32, [c_vp, c_u32, ctypes.POINTER(BatchCfg)])
+
+
+class ServiceCfg(ctypes.Structure):
+    _fields_ = [("shards", c_i32), ("slots", c_i32), ("shard_capacity", c_i64), ("record_bytes", c_u32),
+                ("max_batches_per_launch", c_i32), ("index_budget_bytes", c_i64), ("floor_rows", c_i64)]
+
+
+class ServiceStats(ctypes.Structure):
+    _fields_ = [("submitted", c_i64), ("completed", c_i64), ("rejected", c_i64), ("rows_deleted", c_i64),
+                ("launches", c_i64), ("refills", c_i64), ("rows_appended", c_i64), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("mean_batches_per_launch", ctypes.c_double), ("busy_seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+RZ_SUBMIT_BORROW = 0x1
+_sig("rz_service_create", c_i32, [c_vp, c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(ServiceCfg), ctypes.POINTER(c_vp)])
+_sig("rz_service_submit", c_i32, [c_vp, c_i32, c_vp, c_i64, c_u32, ctypes.POINTER(c_u64)])
+_sig("rz_service_drain", c_i32, [c_vp, c_i32])
+_sig("rz_service_stats_get", c_i32, [c_vp, ctypes.POINTER(ServiceStats)])
+_sig("rz_service_reset_stats", c_i32, [c_vp])
+_sig("rz_service_lengths", c_i32, [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)])
+_sig("rz_service_destroy", None, [c_vp])
+_sig("rz_service_run_poisson", c_i32, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_i64), c_i32, ctypes.c_double,
+                                       ctypes.c_double, c_u64, ctypes.POINTER(ServiceStats)])
+
+_FP = ctypes.POINTER(c_f32)
+_sig("rz_mlp_param_count", c_i32, [])
+_sig("rz_mlp_create", c_i32, [c_vp, c_u64, ctypes.POINTER(c_vp)])
+_sig("rz_mlp_destroy", None, [c_vp])
+_sig("rz_mlp_get_params", c_i32, [c_vp, _FP, c_i32])
+_sig("rz_mlp_set_params", c_i32, [c_vp, _FP, c_i32])
+_sig("rz_mlp_features", c_i32, [c_vp, c_vp, c_i64, c_i64, c_u32, _FP])
+_sig("rz_mlp_forward", c_i32, [c_vp, _FP, c_i64, _FP])
+_sig("rz_mlp_gradients", c_i32, [c_vp, _FP, _FP, c_i64, _FP, _FP])
+_sig("rz_mlp_train", c_i32, [c_vp, _FP, _FP, c_i64, c_i32, c_i32, c_f32, c_u64, _FP])
+_sig("rz_set_predictor", c_i32, [c_vp, c_vp])
+_sig("rz_predict_cfg", c_i32, [c_vp, c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchCfg)])
 _sig("rz_phase_stamps", c_i32, [c_vp, c_i32])
 _sig("rz_read_phase_stamps", c_i32, [c_vp, ctypes.POINTER(c_u64), c_i32, ctypes.POINTER(c_i32)])
 

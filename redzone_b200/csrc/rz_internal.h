@@ -110,6 +110,12 @@ bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* c
 void release_extras(rz_ctx* ctx);
 int read_status(rz_ctx* ctx, cudaStream_t s);
 
+// Batched launches into preallocated scratch (rz_batched.cu), for the streaming service.
+struct BatchArena;
+int arena_create(rz_ctx* ctx, uint32_t w, const rz_batch_cfg* cfg, size_t max_lists, size_t max_k, BatchArena** out);
+void arena_destroy(BatchArena* a);
+int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStream_t s);
+
 // Test hook: run a grid barrier whose expected arrival count exceeds the grid, so that the
 // bounded wait must expire; returns the device status bits observed.
 int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out);

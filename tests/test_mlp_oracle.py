@@ -1,0 +1,45 @@
+"""The predictor's CPU oracle, pinned: its analytic gradient against central finite differences."""
+import numpy as np
+
+from oracle import mlp_ref
+
+
+def random_batch(seed, nb=16):
+    rng = np.random.default_rng(seed)
+    p = rng.normal(0, 0.3, mlp_ref.N_PARAMS)
+    x = rng.uniform(0, 1, (nb, mlp_ref.N_IN))
+    t = rng.uniform(0, 1, (nb, mlp_ref.N_OUT))
+    t[:, : mlp_ref.N_CFG] /= t[:, : mlp_ref.N_CFG].sum(1, keepdims=True)
+    t[:, mlp_ref.N_CFG] = rng.integers(0, 2, nb)
+    return p, x, t
+
+
+def test_analytic_gradient_matches_finite_differences():
+    p, x, t = random_batch(0)
+    _, g = mlp_ref.loss_and_grad(p, x, t)
+    rng = np.random.default_rng(1)
+    # Every bias and a sample of weights from each layer.
+    probe = np.concatenate([np.arange(mlp_ref.OFF_B1, mlp_ref.OFF_W2), np.arange(mlp_ref.OFF_B2, mlp_ref.OFF_W3),
+                            np.arange(mlp_ref.OFF_B3, mlp_ref.N_PARAMS),
+                            rng.integers(mlp_ref.OFF_W1, mlp_ref.OFF_B1, 40),
+                            rng.integers(mlp_ref.OFF_W2, mlp_ref.OFF_B2, 40),
+                            rng.integers(mlp_ref.OFF_W3, mlp_ref.OFF_B3, 40)])
+    h = 1e-6
+    for q in probe:
+        pp, pm = p.copy(), p.copy()
+        pp[q] += h
+        pm[q] -= h
+        fd = (mlp_ref.loss_and_grad(pp, x, t)[0] - mlp_ref.loss_and_grad(pm, x, t)[0]) / (2 * h)
+        assert abs(fd - g[q]) <= 1e-6 + 1e-4 * abs(fd), (q, fd, g[q])
+
+
+def test_features_of_known_patterns():
+    n, k = 1 << 20, 4096
+    run = np.arange(1000, 1000 + k, dtype=np.uint32)  # one run of 4096
+    f = mlp_ref.features(run, n, k, 4)
+    assert f[11] == 1.0 and f[7] == 0.0
+    tail = np.arange(n - k, n, dtype=np.uint32)
+    assert mlp_ref.features(tail, n, k, 4)[6] == 1.0
+    spaced = np.arange(0, n, n // k, dtype=np.uint32)[:k]
+    fs = mlp_ref.features(spaced, n, k, 16)
+    assert fs[7] == 1.0 and abs(fs[4] - 1.0 / 8) < 1e-9 and fs[5] < 1e-12 and fs[3] == 0.5
