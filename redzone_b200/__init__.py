@@ -213,6 +213,86 @@ def remove_batched(ctx: Context, lists, stream=None) -> None:
                                              ctypes.c_void_p(_stream_handle(stream))), "rz_remove_batched")
 
 
+class Service:
+    """Streaming delete service over a device-resident table (rz_service_*).
+
+    ``table`` is a CUDA tensor of shards * shard_capacity records (first axis = records); it must
+    stay alive while the service runs.
+    """
+
+    def __init__(self, ctx: Context, table, shards: int, shard_capacity: int, slots: int = 4,
+                 max_batches_per_launch: int = 32, index_budget_bytes: int = 64 << 20, floor_rows: int = 0,
+                 initial_len=None):
+        self.ctx = ctx
+        self.table = table
+        cfg = _native.ServiceCfg(shards, slots, shard_capacity, item_bytes(table), max_batches_per_launch,
+                                 index_budget_bytes, floor_rows)
+        init = None
+        if initial_len is not None:
+            init = (ctypes.c_int64 * shards)(*[int(x) for x in initial_len])
+        h = ctypes.c_void_p()
+        ctx._check(_native.lib.rz_service_create(ctx.handle, ctypes.c_void_p(table.data_ptr()), init,
+                                                 ctypes.byref(cfg), ctypes.byref(h)), "rz_service_create")
+        self.handle = h
+        self.shards = shards
+        self._lent = []
+
+    def submit(self, shard: int, idx, borrow: bool = False) -> int:
+        """Queue a delete batch (numpy uint32/int32 array or pinned CPU tensor); returns its ticket."""
+        if hasattr(idx, "data_ptr"):
+            ptr, cnt = idx.data_ptr(), int(idx.numel())
+        else:
+            ptr, cnt = idx.ctypes.data, int(idx.size)
+        t = ctypes.c_uint64(0)
+        st = _native.lib.rz_service_submit(self.handle, shard, ctypes.c_void_p(ptr), cnt,
+                                           _native.RZ_SUBMIT_BORROW if borrow else 0, ctypes.byref(t))
+        if borrow:
+            self._lent.append(idx)
+        if st != 0:
+            raise RedzoneError(st, "rz_service_submit")
+        return t.value
+
+    def drain(self, timeout_ms: int = 600000) -> None:
+        self.ctx._check(_native.lib.rz_service_drain(self.handle, timeout_ms), "rz_service_drain")
+        self._lent.clear()
+
+    def stats(self) -> dict:
+        s = _native.ServiceStats()
+        _native.lib.rz_service_stats_get(self.handle, ctypes.byref(s))
+        return s.as_dict()
+
+    def reset_stats(self) -> None:
+        _native.lib.rz_service_reset_stats(self.handle)
+
+    def lengths(self) -> tuple[list[int], list[int]]:
+        """(host view, device-tracked) live lengths per shard."""
+        h = (ctypes.c_int64 * self.shards)()
+        d = (ctypes.c_int64 * self.shards)()
+        self.ctx._check(_native.lib.rz_service_lengths(self.handle, h, d), "rz_service_lengths")
+        return list(h), list(d)
+
+    def run_poisson(self, pool, rate: float, seconds: float, seed: int = 0) -> dict:
+        """Poisson arrivals of random pool batches (pinned CPU tensors) to random shards."""
+        ptrs = (ctypes.c_void_p * len(pool))(*[p.data_ptr() for p in pool])
+        cnts = (ctypes.c_int64 * len(pool))(*[int(p.numel()) for p in pool])
+        s = _native.ServiceStats()
+        self.ctx._check(_native.lib.rz_service_run_poisson(self.handle, ptrs, cnts, len(pool), rate, seconds, seed,
+                                                           ctypes.byref(s)), "rz_service_run_poisson")
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _native.lib.rz_service_destroy(self.handle)
+            self.handle = None
+            self._lent.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 _default: dict[int, Context] = {}
 
 

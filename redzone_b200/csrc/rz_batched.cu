@@ -508,6 +508,168 @@ static int plan_enqueue(rz_batch_plan* plan, cudaStream_t s) {
 
 bool default_batch_cfg(const rz_ctx* ctx, uint32_t w, rz_batch_cfg* cfg);  // rz_autotune.cpp
 
+// ------------------------------------------------------------------------------------------------
+// Arenas: batched launches without per-launch allocation (used by the streaming service). An
+// arena owns device scratch and pinned host staging sized for at most `max_lists` lists with at
+// most `max_k` removals in total; a launch builds its queue and list records in the host staging,
+// uploads them on the launch stream and runs the kernel. The caller must not reuse an arena until
+// its previous launch has completed (the upload reads the staging asynchronously).
+// ------------------------------------------------------------------------------------------------
+struct BatchArena {
+    rz_ctx* ctx = nullptr;
+    uint32_t w = 0;
+    rz_batch_cfg cfg{};
+    uint32_t tile = 0;
+    size_t smem = 0;
+    int grid = 0;
+    size_t max_lists = 0, max_items = 0, max_bits = 0, max_entries = 0, max_cnt = 0;
+    uint8_t* dev = nullptr;
+    uint8_t* host = nullptr;  // pinned
+    size_t off_queue = 0, off_ctr = 0, off_cnt = 0, off_bits = 0, off_dl = 0, off_sl = 0, total = 0;
+};
+
+int arena_create(rz_ctx* ctx, uint32_t w, const rz_batch_cfg* cfg_in, size_t max_lists, size_t max_k,
+                 BatchArena** out) {
+    rz_batch_cfg cfg{};
+    if (cfg_in) cfg = *cfg_in;
+    else default_batch_cfg(ctx, w, &cfg);
+    BatchFn f = batch_fn(int(w), cfg.items);
+    if (!f || max_lists == 0) return RZ_ERR_INVALID_ARG;
+    cudaFuncAttributes fa{};
+    RZ_CUDA_TRY(ctx, cudaFuncGetAttributes(&fa, (const void*)f));
+    cfg.block = std::min(cfg.block, fa.maxThreadsPerBlock & ~31);
+    BatchArena* a = new (std::nothrow) BatchArena();
+    if (!a) return RZ_ERR_NO_MEMORY;
+    a->ctx = ctx;
+    a->w = w;
+    a->cfg = cfg;
+    a->tile = uint32_t(cfg.block) * uint32_t(cfg.items);
+    a->smem = size_t(a->tile / 32 + 2 * a->tile) * 4;
+    a->max_lists = max_lists;
+    const size_t max_tiles = max_k / a->tile + max_lists;  // sum over lists of ceil(k / tile)
+    a->max_items = 3 * max_tiles + max_lists;
+    a->max_bits = max_k / 32 + max_lists;
+    a->max_entries = max_tiles * a->tile;
+    a->max_cnt = 2 * max_tiles;
+    auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+    a->off_queue = up(sizeof(ListRec) * max_lists);
+    a->off_ctr = a->off_queue + up(sizeof(uint2) * a->max_items);
+    a->off_cnt = a->off_ctr + up(4 * (1 + 2 * max_lists));
+    a->off_bits = a->off_cnt + up(4 * a->max_cnt);
+    a->off_dl = a->off_bits + up(4 * a->max_bits);
+    a->off_sl = a->off_dl + up(4 * a->max_entries);
+    a->total = a->off_sl + up(4 * a->max_entries);
+    cudaError_t e = cudaMalloc(&a->dev, a->total);
+    if (e == cudaSuccess) e = cudaMemset(a->dev, 0, a->total);
+    if (e == cudaSuccess) e = cudaMallocHost(&a->host, a->off_ctr);
+    int occ = 0;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(a->smem));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)f, cfg.block, a->smem);
+    if (e != cudaSuccess || occ < 1) {
+        const int st = e != cudaSuccess ? cuda_fail(ctx, e, "arena_create") : RZ_ERR_UNSUPPORTED;
+        if (a->dev) cudaFree(a->dev);
+        if (a->host) cudaFreeHost(a->host);
+        delete a;
+        return st;
+    }
+    a->grid = std::max(1, std::min(cfg.ctas_per_sm, occ) * ctx->sms);
+    *out = a;
+    return RZ_OK;
+}
+
+void arena_destroy(BatchArena* a) {
+    if (!a) return;
+    cudaFree(a->dev);
+    cudaFreeHost(a->host);
+    delete a;
+}
+
+// Build the plan for `lists` into the arena and launch it on `s` (no allocation). Lists must
+// respect the arena's limits (RZ_ERR_UNSUPPORTED otherwise, before anything is enqueued).
+int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStream_t s) {
+    rz_ctx* ctx = a->ctx;
+    if (nlists < 0 || size_t(nlists) > a->max_lists) return RZ_ERR_UNSUPPORTED;
+    ListRec* recs = reinterpret_cast<ListRec*>(a->host);
+    uint2* queue = reinterpret_cast<uint2*>(a->host + a->off_queue);
+    const uint32_t TILE = a->tile;
+    // Count first (so limits are checked before anything is written or enqueued).
+    size_t nmark = 0, nsingle = 0, bits = 0, entries = 0, cnt = 0;
+    for (int l = 0; l < nlists; ++l) {
+        const rz_list_desc& d = lists[l];
+        if (d.n < 0 || d.k < 0 || d.k > d.n || d.n >= (int64_t(1) << 32)) return RZ_ERR_INVALID_ARG;
+        if (d.k == 0 || d.k == d.n) continue;
+        const uint32_t nch = uint32_t((uint64_t(d.k) + TILE - 1) / TILE);
+        if (nch > kMaxTilesPerList) return RZ_ERR_UNSUPPORTED;
+        if (nch == 1) {
+            ++nsingle;
+        } else {
+            const uint32_t span = span_for(nch, a->cfg.span);
+            nmark += (nch + span - 1) / span;
+            bits += (uint64_t(d.k) + 31) / 32;
+            entries += size_t(nch) * TILE;
+            cnt += 2 * size_t(nch);
+        }
+    }
+    if (3 * nmark + nsingle > a->max_items || bits > a->max_bits || entries > a->max_entries || cnt > a->max_cnt)
+        return RZ_ERR_UNSUPPORTED;
+    size_t q_mark = 0, q_single = nmark, q_classify = nmark + nsingle, q_pair = 2 * nmark + nsingle;
+    bits = entries = cnt = 0;
+    for (int l = 0; l < nlists; ++l) {
+        const rz_list_desc& d = lists[l];
+        ListRec r{};
+        r.data = static_cast<uint8_t*>(d.data);
+        r.idx = d.idx;
+        r.n = uint32_t(d.n);
+        r.k = uint32_t(d.k);
+        const uint32_t nch = uint32_t((uint64_t(d.k) + TILE - 1) / TILE);
+        r.nch = nch;
+        if (!(d.k == 0 || d.k == d.n)) {
+            if (nch == 1) {
+                r.span = r.ngroups = 1;
+                queue[q_single++] = make_uint2(uint32_t(l), K_SINGLE << 28);
+            } else {
+                r.span = span_for(nch, a->cfg.span);
+                r.ngroups = (nch + r.span - 1) / r.span;
+                r.bitmap_off = uint32_t(bits);
+                r.list_off = entries;
+                r.cnt_off = uint32_t(cnt);
+                bits += (uint64_t(d.k) + 31) / 32;
+                entries += size_t(nch) * TILE;
+                cnt += 2 * size_t(nch);
+                for (uint32_t g = 0; g < r.ngroups; ++g) {
+                    queue[q_mark++] = make_uint2(uint32_t(l), (K_MARK << 28) | g);
+                    queue[q_classify++] = make_uint2(uint32_t(l), (K_CLASSIFY << 28) | g);
+                    queue[q_pair++] = make_uint2(uint32_t(l), (K_PAIR << 28) | g);
+                }
+            }
+        }
+        recs[l] = r;
+    }
+    const size_t nitems = q_pair;
+    if (nlists > 0)
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(a->dev, a->host, sizeof(ListRec) * size_t(nlists), cudaMemcpyHostToDevice, s));
+    if (nitems)
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(a->dev + a->off_queue, a->host + a->off_queue, sizeof(uint2) * nitems,
+                                         cudaMemcpyHostToDevice, s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(a->dev + a->off_ctr, 0, 4 * (1 + 2 * size_t(nlists)), s));
+    if (nitems == 0) return RZ_OK;
+    BatchParams p;
+    p.lists = reinterpret_cast<const ListRec*>(a->dev);
+    p.queue = reinterpret_cast<const uint2*>(a->dev + a->off_queue);
+    p.nitems = uint32_t(nitems);
+    p.counters = reinterpret_cast<uint32_t*>(a->dev + a->off_ctr);
+    p.chunk_cnt = reinterpret_cast<uint32_t*>(a->dev + a->off_cnt);
+    p.bitmap = reinterpret_cast<uint32_t*>(a->dev + a->off_bits);
+    p.dlist = reinterpret_cast<uint32_t*>(a->dev + a->off_dl);
+    p.slist = reinterpret_cast<uint32_t*>(a->dev + a->off_sl);
+    p.status = ctx->ws.status;
+    p.spin_limit = kSpinLimit;
+    BatchFn f = batch_fn(int(a->w), a->cfg.items);
+    f<<<std::min<int>(a->grid, int(nitems)), a->cfg.block, a->smem, s>>>(p);
+    RZ_CUDA_TRY(ctx, cudaGetLastError());
+    return RZ_OK;
+}
+
 }  // namespace rz
 
 using namespace rz;

@@ -58,8 +58,10 @@ int ensure_seen(rz_ctx* ctx, size_t n) {
 int ensure_partition(rz_ctx* ctx, size_t n, size_t ntiles) {
     int st = grow(ctx, ctx->ws.part_bits, ctx->ws.part_words, (n + 31) / 32 + 1, true);
     if (st != RZ_OK) return st;
-    // Ticket line (16 words) + three 32-bit arrays of ntiles (staged, kept, offset).
-    return grow(ctx, ctx->ws.tile_state, ctx->ws.tile_cap, 16 + (3 * ntiles + 1) / 2 + 1, true);
+    // Ticket line (16 words), three 32-bit arrays of ntiles rounded up to 4 (staged, kept,
+    // offset), then one 16-byte record per tile.
+    const size_t ntp = (ntiles + 3) & ~size_t(3);
+    return grow(ctx, ctx->ws.tile_state, ctx->ws.tile_cap, 16 + 3 * ntp / 2 + 2 * ntiles + 1, true);
 }
 
 int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {

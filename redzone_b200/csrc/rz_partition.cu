@@ -65,9 +65,10 @@ __global__ void partition_count_kernel(const uint32_t* __restrict__ bits, uint32
     }
 }
 
-// Exclusive scan of kept[0..ntiles) into offset[0..ntiles), one CTA of 1024 threads.
+// Exclusive scan of kept[0..ntiles) into offset[0..ntiles) and the per-tile records
+// {offset, kept, 0, 0} the pipelined move copies with each tile; one CTA of 1024 threads.
 __global__ void __launch_bounds__(1024) partition_scan_kernel(const uint32_t* __restrict__ kept, uint32_t ntiles,
-                                                              uint32_t* __restrict__ offset) {
+                                                              uint32_t* __restrict__ offset, uint4* __restrict__ recs) {
     __shared__ uint32_t scratch[33];
     const uint32_t B = blockDim.x;
     const uint32_t per = (ntiles + B - 1) / B;
@@ -77,12 +78,15 @@ __global__ void __launch_bounds__(1024) partition_scan_kernel(const uint32_t* __
     uint32_t total;
     uint32_t run = block_exclusive_scan(s, scratch, &total);
     for (uint32_t t = lo; t < hi; ++t) {
+        const uint32_t c = kept[t];
         offset[t] = run;
-        run += kept[t];
+        recs[t] = make_uint4(run, c, 0u, 0u);
+        run += c;
     }
 }
 
-// One tile per CTA, taken in ticket order.
+// One tile per CTA, taken in ticket order (used for payloads that are not 16-byte aligned, and
+// when phase stamps are on).
 template <int W, int IPT>
 __global__ void __launch_bounds__(kPartBlock) partition_move_kernel(
     uint8_t* data, uint32_t n, uint32_t ntiles, uint32_t* __restrict__ bits, const uint32_t* __restrict__ offset,
@@ -185,161 +189,220 @@ __global__ void __launch_bounds__(kPartBlock) partition_move_kernel(
 }
 
 // ------------------------------------------------------------------------------------------------
-// Move step, pipelined: persistent CTAs (one per SM), kStages tiles of 32 KB in flight per CTA.
-// Thread 0 takes tickets and issues 1-D TMA bulk copies (tile payload + its bitmap words) into a
-// ring of shared-memory stages; a tile's staged flag is raised as soon as its copy has landed
-// (also for tiles still waiting in the ring), so successors waiting on it are not held up by this
-// CTA's processing order. The other threads turn the staged bitmap into ranks and write the kept
-// items out while the next tiles' copies are in flight. Requires a 16-byte-aligned payload.
+// Move step, warp-specialised pipeline: persistent CTAs (one per SM), a ring of kMoveStages
+// shared-memory stages of 32 KB. One producer thread takes tickets (the next one prefetched) and
+// fills free stages with 1-D TMA bulk copies of the tile payload, its bitmap words and its
+// {offset, kept} record; it raises a tile's staged flag as soon as that copy has landed, in issue
+// order, whatever the consumers are doing. Two consumer groups of 8 warps take alternate ring
+// positions, so one group's flag wait and barrier overlap the other group's stores. Inside a
+// group warp w owns a contiguous eighth of the tile: lane j holds the keep word of round j, one
+// warp scan ranks the rounds, one group barrier shares the eight warp totals, and every kept
+// item is written to offset + rank. Every wait is bounded; on expiry the CTA stops consuming, the
+// producer waits (bounded) for its copies in flight, and the status word gets ST_TIMEOUT.
+// Requires a 16-byte-aligned payload.
 // ------------------------------------------------------------------------------------------------
-constexpr int kStages = 4;
+constexpr int kMoveStages = 6;
 constexpr uint32_t kTileBytes = 32768;
-constexpr int kTmaBlock = 256;
+constexpr int kMoveGroups = 2;
+constexpr int kGroupThreads = 256;
+constexpr int kMoveBlock = kMoveGroups * kGroupThreads + 32;
 
 template <int W>
-__global__ void __launch_bounds__(kTmaBlock, 1) partition_move_tma_kernel(
-    uint8_t* data, uint32_t n, uint32_t ntiles, uint32_t* __restrict__ bits, const uint32_t* __restrict__ offset,
+constexpr size_t move_smem_bytes() {
+    return size_t(kMoveStages) * kTileBytes + size_t(kMoveStages) * (kTileBytes / W / 8) + size_t(kMoveStages) * 16;
+}
+
+template <int W>
+__global__ void __launch_bounds__(kMoveBlock, 1) partition_move_ws_kernel(
+    uint8_t* data, uint32_t n, uint32_t ntiles, uint32_t* __restrict__ bits, const uint4* __restrict__ recs,
     uint32_t* staged, unsigned long long* ticket, uint32_t tag, uint32_t* status, uint32_t spin_limit,
     unsigned long long* dev_len, uint32_t new_len) {
     using T = typename Payload<W>::T;
-    constexpr uint32_t TILE = kTileBytes / W;   // items per tile
-    constexpr uint32_t BW = TILE / 32;          // bitmap words per tile
-    constexpr int B = kTmaBlock, NW = B / 32;
-    constexpr int ROUNDS = TILE / B;            // items per thread per tile
+    constexpr uint32_t TILE = kTileBytes / W;  // items per tile
+    constexpr uint32_t BW = TILE / 32;         // bitmap words per tile
+    constexpr int S = kMoveStages;
+    constexpr int GW = kGroupThreads / 32;     // warps per consumer group
+    constexpr uint32_t PER_WARP = TILE / GW;   // items per warp and tile
+    constexpr int R = int(PER_WARP / 32);      // rounds per warp = bitmap words per warp
+    static_assert(R >= 1 && R <= 32, "one keep word per lane");
     T* A = reinterpret_cast<T*>(data);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     extern __shared__ __align__(128) uint8_t smem[];
-    T* stage = reinterpret_cast<T*>(smem);                                       // [kStages][TILE]
-    uint32_t* sbits = reinterpret_cast<uint32_t*>(smem + kStages * kTileBytes);  // [kStages][BW]
-    __shared__ __align__(8) unsigned long long bars[kStages];
-    __shared__ uint32_t s_tile[kStages];
-    __shared__ uint32_t s_cnt[ROUNDS * NW + 1];
-    if (blockIdx.x == 0 && threadIdx.x == 0 && dev_len) *dev_len = new_len;
+    T* stage = reinterpret_cast<T*>(smem);                                   // [S][TILE]
+    uint32_t* sbits = reinterpret_cast<uint32_t*>(smem + S * kTileBytes);    // [S][BW]
+    uint4* srec = reinterpret_cast<uint4*>(smem + S * kTileBytes + S * BW * 4);  // [S]
+    __shared__ __align__(8) unsigned long long full[S], empty[S];
+    __shared__ uint32_t s_tile[S];
+    __shared__ uint32_t s_wtot[kMoveGroups][GW];
+    __shared__ uint32_t s_go[kMoveGroups][2];  // [group][barrier A / barrier B] outcome
+    __shared__ volatile uint32_t s_abort;
 
-    uint32_t published = 0;  // thread 0: stages whose staged flag is raised for the current tile
-    auto issue = [&](int s) {  // thread 0: refill stage s with the next ticket
-        const uint32_t t = uint32_t(atomicAdd(ticket, 1ull));
-        s_tile[s] = t;
-        published &= ~(1u << s);
-        if (t >= ntiles) return;
-        const uint32_t base = t * TILE;
-        const uint32_t items = min(TILE, n - base);
-        const uint32_t bulk = (items * W) & ~15u;
-        mbar_arrive_expect_tx(&bars[s], bulk + BW * 4);
-        if (bulk) tma_load_1d(stage + size_t(s) * TILE, data + size_t(base) * W, bulk, &bars[s]);
-        tma_load_1d(sbits + s * BW, bits + size_t(t) * BW, BW * 4, &bars[s]);
-    };
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], GW);
+        }
+        s_abort = 0u;
         fence_mbar_init();
-        for (int s = 0; s < kStages; ++s) issue(s);
+        if (blockIdx.x == 0 && dev_len) *dev_len = new_len;
     }
     __syncthreads();
 
-    uint32_t parity = 0;  // bit s: phase parity of stage s
-    int timed_out = 0;
-    for (int s = 0;; s = (s + 1 == kStages) ? 0 : s + 1) {
-        const uint32_t t = s_tile[s];
-        if (t >= ntiles) break;  // tickets grow along the ring, so every later stage is empty too
-        const uint32_t base = t * TILE;
-        const uint32_t items = min(TILE, n - base);
-        // Wait for this stage's copy (bounded; a copy of valid memory always lands).
-        {
+    if (warp == kMoveGroups * GW) {
+        // ---------------- producer ----------------
+        if (lane != 0) return;
+        uint32_t issued = 0, pub = 0, ends = 0, idle = 0;
+        bool done = false;
+        unsigned long long next = atomicAdd(ticket, 1ull);
+        while (true) {
+            bool prog = false;
+            // Raise the staged flags of landed copies, in issue order.
+            while (pub < issued) {
+                const int s = int(pub % S);
+                if (!mbar_test_wait(&full[s], (pub / S) & 1u)) break;
+                const uint32_t t = s_tile[s];
+                if (t < ntiles) st_relaxed(&staged[t], tag);
+                ++pub;
+                prog = true;
+            }
+            if (s_abort) break;
+            if (ends < uint32_t(kMoveGroups)) {
+                const uint32_t p = issued;
+                const int s = int(p % S);
+                // A stage is free once its previous position is published and consumed.
+                const bool free = p < uint32_t(S) || (pub + S > p && mbar_test_wait(&empty[s], ((p / S) - 1u) & 1u));
+                if (free) {
+                    fence_proxy_async_smem();  // the consumers' generic reads of the stage come first
+                    const uint32_t t = done ? ntiles : uint32_t(min(next, (unsigned long long)ntiles));
+                    s_tile[s] = t;
+                    if (t < ntiles) {
+                        next = atomicAdd(ticket, 1ull);  // prefetch: used at the next issue
+                        const uint32_t base = t * TILE;
+                        const uint32_t items = min(TILE, n - base);
+                        const uint32_t bulk = (items * W) & ~15u;
+                        mbar_arrive_expect_tx(&full[s], bulk + BW * 4 + 16);
+                        if (bulk) tma_load_1d(stage + size_t(s) * TILE, data + size_t(base) * W, bulk, &full[s]);
+                        tma_load_1d(sbits + s * BW, bits + size_t(t) * BW, BW * 4, &full[s]);
+                        tma_load_1d(&srec[s], recs + t, 16, &full[s]);
+                    } else {
+                        done = true;
+                        ++ends;
+                        mbar_arrive(&full[s]);  // end marker: completes the phase with no bytes
+                    }
+                    ++issued;
+                    prog = true;
+                }
+            } else if (pub == issued) {
+                break;
+            }
+            if (prog) {
+                idle = 0;
+            } else if (++idle > spin_limit) {
+                s_abort = 1u;
+                atomicOr(status, ST_TIMEOUT);
+                break;
+            }
+        }
+        // Never leave with copies in flight into this CTA's shared memory.
+        for (; pub < issued; ++pub) {
             uint32_t it = 0;
-            while (!mbar_try_wait(&bars[s], (parity >> s) & 1u)) {
-                if (++it > spin_limit) {
-                    timed_out = 1;
+            while (!mbar_test_wait(&full[pub % S], (pub / S) & 1u) && ++it <= spin_limit) {
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    const int g = warp / GW, gw = warp % GW;
+    const int gt = threadIdx.x - g * kGroupThreads;
+    const uint32_t bar_id = 1u + uint32_t(g);
+    const uint32_t lt = lanemask_lt();
+    for (uint32_t p = uint32_t(g);; p += kMoveGroups) {
+        const int s = int(p % S);
+        const uint32_t par = (p / S) & 1u;
+        // One thread waits (bounded) for the stage; the group learns the outcome at the barrier.
+        if (gt == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            while (!mbar_try_wait(&full[s], par)) {
+                if (s_abort || ++it > spin_limit) {
+                    ok = false;
                     break;
                 }
             }
-            parity ^= 1u << s;
+            if (!ok && !s_abort) {
+                s_abort = 1u;
+                atomicOr(status, ST_TIMEOUT);
+            }
+            s_go[g][0] = ok ? 1u : 0u;
         }
+        named_bar(bar_id, kGroupThreads);
+        if (!s_go[g][0]) break;
+        mbar_try_wait(&full[s], par);  // completed: acquires the copied bytes for this thread
+        const uint32_t t = s_tile[s];
+        if (t >= ntiles) break;
+        const uint32_t base = t * TILE;
+        const uint32_t items = min(TILE, n - base);
+        const uint4 rec = srec[s];
+        const uint32_t off = rec.x, total = rec.y;
         T* st = stage + size_t(s) * TILE;
-        const uint32_t* sb = sbits + s * BW;
         // The ragged end of the last tile (fewer than 16 bytes) comes through plain loads.
         const uint32_t bulk_items = ((items * W) & ~15u) / W;
-        for (uint32_t q = bulk_items + threadIdx.x; q < items; q += B) st[q] = A[base + q];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            // This tile's input is read; so is that of every other stage whose copy has landed,
-            // except a last tile with a ragged end (read by plain loads when it is processed).
-            if (!(published & (1u << s))) st_release(&staged[t], tag);
-            const bool last_ragged = ((n - (ntiles - 1) * TILE) * W) % 16 != 0;
-            for (int o = 1; o < kStages; ++o) {
-                const int so = (s + o) % kStages;
-                const uint32_t to = s_tile[so];
-                if (to >= ntiles || (published & (1u << so))) continue;
-                if (last_ragged && to == ntiles - 1) continue;
-                if (mbar_try_wait(&bars[so], (parity >> so) & 1u)) {
-                    st_release(&staged[to], tag);
-                    published |= 1u << so;
-                }
-            }
+        for (uint32_t q = bulk_items + uint32_t(gt); q < items; q += kGroupThreads) st[q] = A[base + q];
+        // Keep word of round `lane` of this warp (bits past n are not items).
+        uint32_t kw = 0u;
+        if (lane < R) {
+            const uint32_t wi = uint32_t(gw) * R + uint32_t(lane);
+            const uint32_t first = base + wi * 32u;
+            const uint32_t valid = first >= n ? 0u : (n - first >= 32u ? 0xffffffffu : (1u << (n - first)) - 1u);
+            kw = ~sbits[s * BW + wi] & valid;
+            bits[size_t(t) * BW + wi] = 0u;  // leave the removal map zero for the next call
         }
-        // Ranks of the kept items, round-major (round j covers items j*B .. j*B+B-1).
-        uint32_t km[ROUNDS];
-#pragma unroll
-        for (int j = 0; j < ROUNDS; ++j) {
-            const uint32_t q = uint32_t(j) * B + threadIdx.x;
-            const bool keep = q < items && ((sb[q >> 5] >> (q & 31u)) & 1u) == 0u;
-            km[j] = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) s_cnt[j * NW + warp] = __popc(km[j]);
-        }
-        // Leave the removal map zero for the next call (coalesced: one word per thread).
-        for (uint32_t q = threadIdx.x; q < BW; q += B)
-            if (base + q * 32 < n) bits[size_t(t) * BW + q] = 0u;
-        __syncthreads();
-        const uint32_t off = __ldg(&offset[t]);
-        if (warp == 0) {
-            constexpr int E = ROUNDS * NW;
-            constexpr int per = (E + 31) / 32;
-            const int lo = lane * per, hi = min(lo + per, E);
-            uint32_t sum = 0;
-            for (int e = lo; e < hi; ++e) sum += s_cnt[e];
-            const uint32_t inc = warp_inclusive_scan(sum);
-            uint32_t run = inc - sum;
-            for (int e = lo; e < hi; ++e) {
-                const uint32_t x = s_cnt[e];
-                s_cnt[e] = run;
-                run += x;
-            }
-            const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-            // Wait for the (at most two) tiles whose input this tile's output overlaps.
-            if (total > 0 && lane < 2) {
+        const uint32_t c = __popc(kw);
+        const uint32_t inc = warp_inclusive_scan(c);
+        if (lane == 31) s_wtot[g][gw] = inc;
+        // Wait for the (at most two) tiles whose input this tile's output overlaps.
+        if (gw == 0) {
+            if (lane < 2 && total > 0) {
                 const uint32_t u = off / TILE + uint32_t(lane);
-                if (u <= (off + total - 1) / TILE && u < t) {
+                if (u <= (off + total - 1u) / TILE && u < t) {
                     uint32_t it = 0;
                     while (ld_acquire(&staged[u]) != tag) {
-                        if (++it > spin_limit) {
-                            timed_out = 1;
+                        if (s_abort || ++it > spin_limit) {
+                            if (!s_abort) atomicOr(status, ST_TIMEOUT);
+                            s_abort = 1u;
                             break;
                         }
                     }
                 }
             }
+            __syncwarp();
+            if (lane == 0) s_go[g][1] = s_abort ? 0u : 1u;
         }
-        __syncthreads();
-        const uint32_t lt = lanemask_lt();
+        named_bar(bar_id, kGroupThreads);
+        if (!s_go[g][1]) break;
+        uint32_t wpre = 0;
 #pragma unroll
-        for (int j = 0; j < ROUNDS; ++j) {
-            const uint32_t q = uint32_t(j) * B + threadIdx.x;
-            if ((km[j] >> lane) & 1u) A[off + s_cnt[j * NW + warp] + __popc(km[j] & lt)] = st[q];
+        for (int q = 0; q < GW; ++q) wpre += q < gw ? s_wtot[g][q] : 0u;
+        const uint32_t excl = inc - c;
+        const T* src = st + size_t(gw) * PER_WARP;
+        const uint32_t dst0 = off + wpre;
+#pragma unroll 8
+        for (int j = 0; j < R; ++j) {
+            const uint32_t km = __shfl_sync(0xffffffffu, kw, j);
+            const uint32_t ej = __shfl_sync(0xffffffffu, excl, j);
+            if ((km >> lane) & 1u) A[dst0 + ej + __popc(km & lt)] = src[j * 32 + lane];
         }
-        __syncthreads();  // stage s is consumed
-        if (threadIdx.x == 0) {
-            fence_proxy_async_smem();  // generic reads of the stage precede the next async write
-            issue(s);
-        }
-        __syncthreads();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
     }
-    if (timed_out) atomicOr(status, ST_TIMEOUT);
 }
 
 using MoveFn = void (*)(uint8_t*, uint32_t, uint32_t, uint32_t*, const uint32_t*, uint32_t*, unsigned long long*,
                         uint32_t, uint32_t*, uint32_t, unsigned long long*, uint32_t, unsigned long long*, uint32_t);
-using MoveTmaFn = void (*)(uint8_t*, uint32_t, uint32_t, uint32_t*, const uint32_t*, uint32_t*, unsigned long long*,
-                           uint32_t, uint32_t*, uint32_t, unsigned long long*, uint32_t);
+using MoveWsFn = void (*)(uint8_t*, uint32_t, uint32_t, uint32_t*, const uint4*, uint32_t*, unsigned long long*,
+                          uint32_t, uint32_t*, uint32_t, unsigned long long*, uint32_t);
 
 // 32 KB of payload per tile for every width.
 static int part_items(int w) { return w == 4 ? 16 : w == 8 ? 8 : w == 16 ? 4 : 2; }
@@ -351,12 +414,12 @@ static MoveFn move_fn(int w) {
         default: return partition_move_kernel<32, 2>;
     }
 }
-static MoveTmaFn move_tma_fn(int w) {
+static MoveWsFn move_ws_fn(int w, size_t* smem) {
     switch (w) {
-        case 4: return partition_move_tma_kernel<4>;
-        case 8: return partition_move_tma_kernel<8>;
-        case 16: return partition_move_tma_kernel<16>;
-        default: return partition_move_tma_kernel<32>;
+        case 4: *smem = move_smem_bytes<4>(); return partition_move_ws_kernel<4>;
+        case 8: *smem = move_smem_bytes<8>(); return partition_move_ws_kernel<8>;
+        case 16: *smem = move_smem_bytes<16>(); return partition_move_ws_kernel<16>;
+        default: *smem = move_smem_bytes<32>(); return partition_move_ws_kernel<32>;
     }
 }
 
@@ -371,24 +434,27 @@ int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint
     st = reset_if_dirty(ctx, s);
     if (st != RZ_OK) return st;
     const bool validate = (flags & RZ_VALIDATE) != 0;
-    // Scratch layout in tile_state: the ticket on its own 128-byte line, then staged[ntiles],
-    // kept[ntiles] and offset[ntiles] as 32-bit arrays. Ticket and staged flags are cleared by
-    // one memset per call (which keeps the call correct when it is replayed from a CUDA graph).
+    // Scratch layout in tile_state: the ticket on its own 128-byte line, then staged, kept and
+    // offset as 32-bit arrays of ntiles rounded up to a multiple of 4, then the 16-byte records.
+    // Ticket and staged flags are cleared by one memset per call (which keeps the call correct
+    // when it is replayed from a CUDA graph).
+    const uint32_t ntp = (ntiles + 3u) & ~3u;
     unsigned long long* ticket = ctx->ws.tile_state;
     uint32_t* staged = reinterpret_cast<uint32_t*>(ctx->ws.tile_state + 16);
-    uint32_t* kept = staged + ntiles;
-    uint32_t* offset = kept + ntiles;
+    uint32_t* kept = staged + ntp;
+    uint32_t* offset = kept + ntp;
+    uint4* recs = reinterpret_cast<uint4*>(offset + ntp);
     const uint32_t tag = 1u;
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(ticket, 0, 128 + size_t(ntiles) * 4, s));
     const int mgrid = std::max(1, std::min<int>(ctx->sms * 8, int((k + 255) / 256)));
     partition_mark_kernel<<<mgrid, 256, 0, s>>>(idx, k, n, ctx->ws.part_bits, ctx->ws.status, validate ? 1u : 0u);
     const int cgrid = std::max(1, std::min<int>(ctx->sms * 8, int((ntiles + 7) / 8)));
     partition_count_kernel<<<cgrid, 256, 0, s>>>(ctx->ws.part_bits, n, tile, ntiles, kept);
-    partition_scan_kernel<<<1, 1024, 0, s>>>(kept, ntiles, offset);
+    partition_scan_kernel<<<1, 1024, 0, s>>>(kept, ntiles, offset, recs);
     int grid = int(ntiles), block = kPartBlock;
     if ((reinterpret_cast<uintptr_t>(data) & 15u) == 0 && !ctx->ws.stamps_on) {
-        MoveTmaFn f = move_tma_fn(int(w));
-        const size_t smem = size_t(kStages) * kTileBytes + size_t(kStages) * (kTileBytes / w / 8);
+        size_t smem = 0;
+        MoveWsFn f = move_ws_fn(int(w), &smem);
         static bool attr_set[4] = {false, false, false, false};
         const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
         if (!attr_set[wi]) {
@@ -396,8 +462,8 @@ int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint
             attr_set[wi] = true;
         }
         grid = std::max(1, std::min<int>(ctx->sms, int(ntiles)));
-        block = kTmaBlock;
-        f<<<grid, kTmaBlock, smem, s>>>(static_cast<uint8_t*>(data), n, ntiles, ctx->ws.part_bits, offset, staged,
+        block = kMoveBlock;
+        f<<<grid, kMoveBlock, smem, s>>>(static_cast<uint8_t*>(data), n, ntiles, ctx->ws.part_bits, recs, staged,
                                          ticket, tag, ctx->ws.status, kSpinLimit, ctx->ws.dev_len, n - k);
     } else {
         const uint32_t stride = std::max<uint32_t>(1u, (ntiles + kMaxGrid - 1) / kMaxGrid);

@@ -174,6 +174,22 @@ def test_partition_matches_stable_oracle(ctx):
             assert np.array_equal(got[: n - k], exp[: n - k]), (words, n, k)
 
 
+def test_partition_many_tiles_per_cta(ctx):
+    """Thousands of 32 KB tiles (several per CTA through the stage ring), clustered and uniform
+    removals, a ragged end, and back-to-back calls on the same context (map left zero)."""
+    cases = [(1, (1 << 24) + 5, "uniform", 1 << 16), (1, 1 << 24, "clustered", 1 << 22),
+             (2, (1 << 22) + 3, "tail", 1 << 18), (4, 1 << 21, "uniform", 1 << 20)]
+    for words, n, dist, k in cases:
+        host = payload(n, words, seed=words + 7)
+        idx = workloads.make(dist, n, k, seed=k)
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        ctx.partition(d, torch.from_numpy(idx.astype(np.int32)).to(DEV), flags=rz.RZ_SYNC)
+        exp = host.copy()
+        oracle.stable_remove(exp, idx)
+        got = d.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got[: n - k], exp[: n - k]), (words, n, dist, k)
+
+
 def test_bounded_barrier_wait_times_out_with_status(ctx):
     bits = ctx.test_barrier_timeout(spin_limit=2000)
     assert bits & 4
