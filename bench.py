@@ -263,6 +263,31 @@ def own_arm(args):
     region_ms = max_over_ranks(region0.elapsed_time(region1))
     value = world * k / (mean_ms * 1e-3)
 
+    # ---- steady state: one CUDA graph of NSETS x [removal, L2 scrub] replayed back to back, minus
+    # the same graph with the scrubs alone (no per-step event or launch gaps) ----
+    graphs = []
+    for with_remove in (True, False):
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr):
+            for i in range(NSETS):
+                if with_remove:
+                    ctx.remove(a, sets[i])
+                scrub.fill_(i & 255)
+        graphs.append(gr)
+    reps = max(3, min(200, args.steps // NSETS))
+    g_ms = []
+    for gr in graphs:
+        gr.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            gr.replay()
+        e1.record(stream)
+        e1.synchronize()
+        g_ms.append(e0.elapsed_time(e1))
+    del graphs
+    steady_ms = max_over_ranks(max(1e-6, (g_ms[0] - g_ms[1]) / (reps * NSETS)))
+
     # ---- O(n) partition comparator on the same workload (fewer steps; ~1 GiB read + write each) ----
     p_steps = max(5, min(50, args.steps // 20))
     p_ms = []
@@ -318,6 +343,11 @@ def own_arm(args):
                          "alg_bytes_per_launch": balg, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6.65 TB/s"},
             "partition_on": {"ms_per_step": part_ms, "speedup_redzone_vs_partition": part_ms / mean_ms},
+            "graph_steady_state": {
+                "ms_per_removal": steady_ms, "items_per_s": world * k / (steady_ms * 1e-3),
+                "speedup_vs_partition": part_ms / steady_ms,
+                "method": f"CUDA graph of {NSETS} x [removal, 256 MiB scrub] replayed {reps} times, minus the "
+                          f"same graph of scrubs alone, divided by the removals"},
             "e2e": {"value": world * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 4 * k,
                     "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms},
             "cpu_baseline": cpu,

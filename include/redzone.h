@@ -112,9 +112,20 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
                        rz_stream_t stream);
 
 /*
- * O(n) stable partition comparator (mark + single-pass decoupled look-back compaction), in
- * place. Survivors keep their relative order, as with thrust::remove (Thrust_remove.hxx:15-17)
- * and InK compact (cuCompactor.cuh:104-141).
+ * Add-then-remove (the paper's growth step, Sec. 4.6): append g items from d_gain (device) at
+ * rows [n, n + g) of d_data, whose allocation must hold capacity >= n + g items, then remove the k
+ * distinct rows d_idx (each < n + g, so appended rows may be removed too) from the grown list with
+ * the Redzone rule. *new_len = n + g - k. No counterpart in the reference's code; it replaces a
+ * caller's copy followed by RemoveFromList_GPUWide (redzone.hxx:626) on Length + g.
+ */
+int rz_append_remove(rz_ctx* ctx, void* d_data, int64_t n, int64_t capacity, uint32_t elem_bytes,
+                     const void* d_gain, int64_t g, const uint32_t* d_idx, int64_t k, int64_t* new_len,
+                     uint32_t flags, rz_stream_t stream);
+
+/*
+ * O(n) stable partition comparator (mark, per-tile counts and their scan, then a pipelined
+ * in-place move), in place. Survivors keep their relative order, as with thrust::remove
+ * (Thrust_remove.hxx:15-17) and InK compact (cuCompactor.cuh:104-141).
  */
 int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
                  const uint32_t* d_idx, int64_t k, int64_t* new_len, uint32_t flags,

@@ -97,6 +97,18 @@ class Context:
                                        ctypes.c_void_p(_stream_handle(stream)))
         self._check(st, "rz_remove_cfg")
 
+    def append_remove(self, data, n: int, gain, idx, flags: int = 0, stream=None) -> int:
+        """Append `gain` (device tensor of items) at rows [n, n + g) of `data` (capacity =
+        data.shape[0]), then remove rows `idx` from the grown list; returns n + g - k."""
+        g, k = int(gain.shape[0]), int(idx.numel())
+        out = ctypes.c_int64(0)
+        st = _native.lib.rz_append_remove(self.handle, ctypes.c_void_p(data.data_ptr()), n, int(data.shape[0]),
+                                          item_bytes(data), ctypes.c_void_p(gain.data_ptr()), g,
+                                          ctypes.c_void_p(idx.data_ptr()), k, ctypes.byref(out), flags,
+                                          ctypes.c_void_p(_stream_handle(stream)))
+        self._check(st, "rz_append_remove")
+        return out.value
+
     def partition(self, data, idx, flags: int = 0, stream=None) -> int:
         """O(n) stable partition comparator (survivors keep their order)."""
         n, k = int(data.shape[0]), int(idx.numel())

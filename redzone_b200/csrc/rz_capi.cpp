@@ -273,6 +273,22 @@ int rz_remove(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const u
     return rz_remove_cfg(ctx, d_data, n, elem_bytes, d_idx, k, &cfg, flags, stream);
 }
 
+int rz_append_remove(rz_ctx* ctx, void* d_data, int64_t n, int64_t capacity, uint32_t elem_bytes,
+                     const void* d_gain, int64_t g, const uint32_t* d_idx, int64_t k, int64_t* new_len,
+                     uint32_t flags, rz_stream_t stream) {
+    if (!ctx || g < 0 || n < 0 || (g > 0 && !d_gain) || capacity < n + g) return RZ_ERR_INVALID_ARG;
+    int st = check_args(d_data, n + g, elem_bytes, d_idx, k);
+    if (st != RZ_OK) return st;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (g > 0) {
+        uint8_t* dst = static_cast<uint8_t*>(d_data) + size_t(n) * elem_bytes;
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(dst, d_gain, size_t(g) * elem_bytes, cudaMemcpyDeviceToDevice,
+                                         reinterpret_cast<cudaStream_t>(stream)));
+    }
+    return rz_remove(ctx, d_data, n + g, elem_bytes, d_idx, k, new_len, flags, stream);
+}
+
 int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
                  int64_t* new_len, uint32_t flags, rz_stream_t stream) {
     if (!ctx) return RZ_ERR_INVALID_ARG;

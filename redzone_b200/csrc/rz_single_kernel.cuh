@@ -166,7 +166,9 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
             if (lane == 0) cbuf[j * nw + warp] = (uint32_t(__popc(dmask[j])) << 16) | uint32_t(__popc(smask[j]));
         }
         // Clear the bitmap words of this tile (lane 0 owns the 32 items of its warp and round).
-        if (lane == 0) {
+        // With one tile per CTA the clear waits until the counts are published (below), so the
+        // publishing release does not wait for these stores either.
+        if (!single && lane == 0) {
 #pragma unroll
             for (int j = 0; j < IPT; ++j) {
                 const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
@@ -174,6 +176,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
             }
         }
         __syncthreads();
+        if (tt == 0) RZ_STAMP(p, 6);
         if (warp == 0) {
             const int per = (E + 31) >> 5;
             const int lo = lane * per, hi = min(lo + per, E);
@@ -202,7 +205,14 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
                 }
                 if (sv[j] && !dv[j]) {
                     const uint32_t rank = (ex & 0xffffu) + __popc(smask[j] & lt);
-                    p.slist[chunk_base + scnt + rank] = cut + i;
+                    // 4-byte items with one tile per CTA: the list holds the source item itself
+                    // (already in registers; tail items are never written), which saves phase C
+                    // a dependent load. Otherwise it holds the source position.
+                    if constexpr (W == 4) {
+                        p.slist[chunk_base + scnt + rank] = single ? uint32_t(src[j]) : cut + i;
+                    } else {
+                        p.slist[chunk_base + scnt + rank] = cut + i;
+                    }
                 }
             }
         }
@@ -224,6 +234,13 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
 #pragma unroll
         for (int j = 0; j < IPT; ++j)
             if (dv[j] && sv[j]) head[rr[j]] = src[j];
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const uint32_t i = t0 * TILE + uint32_t(j) * B + threadIdx.x;
+                if (i < k) p.bitmap[i >> 5] = 0u;
+            }
+        }
     }
     if (G > 1) {
         if (dcnt == 0u) {
@@ -250,6 +267,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
         }
         if (threadIdx.x == 0) fence_acq_rel_gpu();  // the other CTAs' source-orphan lists
         __syncthreads();
+        RZ_STAMP(p, 7);
         block_scan_array(s_pd, int(G), s_scan);
         block_scan_array(s_ps, int(G), s_scan);
     } else {
@@ -273,9 +291,13 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
         }
         const int c2 = owner_of_rank(s_ps, int(G), jr);
         const uint32_t base2 = min(uint32_t(c2) * tpc, ntiles) * TILE;
-        const uint32_t pos = __ldcg(&p.slist[base2 + (jr - s_ps[c2])]);
+        const uint32_t ent = __ldcg(&p.slist[base2 + (jr - s_ps[c2])]);
         const uint32_t dest = __ldcg(&p.dlist[chunk_base + r]);
-        head[dest] = reinterpret_cast<const T*>(p.data)[pos];
+        if constexpr (W == 4) {
+            head[dest] = single ? T(ent) : reinterpret_cast<const T*>(p.data)[ent];
+        } else {
+            head[dest] = reinterpret_cast<const T*>(p.data)[ent];
+        }
     }
     RZ_STAMP(p, 4);
 }

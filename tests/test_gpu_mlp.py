@@ -1,4 +1,5 @@
 """GPU checks of the learned predictor's hand-written kernels against the CPU oracle."""
+import ctypes
 import numpy as np
 import pytest
 import torch
@@ -94,3 +95,53 @@ def test_predicted_configuration_keeps_results_bit_exact(ctx):
         oracle.remove(exp, idx)
         assert np.array_equal(d.cpu().numpy().view(np.uint32)[: n - k], exp[: n - k])
     m.close()
+
+
+def test_shipped_predictor_on_the_gpu_matches_the_oracle_and_its_regret(ctx):
+    """The shipped weights run through the library's own forward kernel: predictions agree with the
+    CPU oracle (up to near-ties) and keep the held-out regret within 5 % of exhaustive autotune."""
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    p = np.load(root / "redzone_b200" / "data" / "predictor.npz")["params"]
+    h = np.load(root / "tests" / "golden" / "predictor_heldout.npz")
+    X, T, dcls = h["X"], h["T"], h["default_cls"]
+    m = learn.Mlp(ctx)
+    m.set_params(p)
+    cls, bit = m.predict(X)
+    _, _, ref = mlp_ref.forward(p.astype(np.float64), X.astype(np.float64))
+    agree = cls == ref[:, : mlp_ref.N_CFG].argmax(1)
+    assert agree.mean() > 0.99
+    rep = learn.evaluate(cls, bit, T, dcls)
+    assert rep["regret_mean"] <= 0.05 and rep["regret_mean"] < rep["default_regret_mean"]
+    m.close()
+
+
+def test_attached_predictor_is_used_and_falls_back(ctx):
+    """rz_remove with RZ_USE_PREDICTOR runs the network's configuration; without a network
+    attached the same flag falls back to the tables / defaults. Results are bit-exact either way."""
+    n, k = 1 << 20, 1 << 14
+    host = np.arange(n, dtype=np.uint32)
+    idx = workloads.uniform(n, k, seed=5)
+    exp = host.copy()
+    oracle.remove(exp, idx)
+    d_idx = torch.from_numpy(idx.astype(np.int32)).to(DEV)
+    for attach in (True, False):
+        c = rz.Context(0)
+        m = learn.attach_default(c) if attach else None
+        assert (m is not None) == attach
+        cfg = rz.LaunchCfg()
+        st = rz._native.lib.rz_predict_cfg(c.handle, ctypes.c_void_p(d_idx.data_ptr()), n, k, 4, ctypes.byref(cfg))
+        if attach:
+            assert st == 0
+            p = np.load(learn.DATA / "predictor.npz")["params"].astype(np.float64)
+            _, _, o = mlp_ref.forward(p, mlp_ref.features(idx, n, k, 4)[None, :].astype(np.float64))
+            q = learn.config_space().index((cfg.block, cfg.items, cfg.ctas_per_sm))
+            assert o[0, q] >= o[0, : mlp_ref.N_CFG].max() - 1e-3  # the oracle's choice, up to a near-tie
+        else:
+            assert st == rz._native.RZ_ERR_UNSUPPORTED  # no network: rz_remove falls back to the tables
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        c.remove(d, torch.from_numpy(idx.astype(np.int32)).to(DEV), flags=rz.RZ_USE_PREDICTOR | rz.RZ_SYNC)
+        assert np.array_equal(d.cpu().numpy().view(np.uint32)[: n - k], exp[: n - k])
+        if m is not None:
+            m.close()
+        c.close()

@@ -190,6 +190,25 @@ def test_partition_many_tiles_per_cta(ctx):
         assert np.array_equal(got[: n - k], exp[: n - k]), (words, n, dist, k)
 
 
+def test_append_then_remove(ctx):
+    """Gains appended at the tail, then removal over the grown list (appended rows removable)."""
+    for words, n, g, k in [(1, 1 << 18, 1 << 12, 1 << 13), (4, 5000, 300, 2000), (2, 1 << 16, 0, 100)]:
+        cap = n + g + 17
+        host = payload(cap, words, seed=n)
+        gain = payload(g, words, seed=g + 1) if g else np.zeros((0, words), np.uint32)
+        gain[:, 0] = 0xF0000000 + np.arange(g, dtype=np.uint32)
+        idx = workloads.uniform(n + g, k, seed=k)
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        dg = torch.from_numpy(gain.view(np.int32).copy()).to(DEV)
+        new_len = ctx.append_remove(d, n, dg, torch.from_numpy(idx.astype(np.int32)).to(DEV), flags=rz.RZ_SYNC)
+        assert new_len == n + g - k
+        grown = np.concatenate([host[:n], gain])
+        oracle.remove(grown, idx)
+        got = d.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got[:new_len], grown[:new_len]), (words, n, g, k)
+        assert np.array_equal(got[n + g:], host[n + g:])  # past the grown list: untouched
+
+
 def test_bounded_barrier_wait_times_out_with_status(ctx):
     bits = ctx.test_barrier_timeout(spin_limit=2000)
     assert bits & 4
