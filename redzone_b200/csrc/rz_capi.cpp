@@ -48,6 +48,7 @@ int ensure_lists(rz_ctx* ctx, size_t k) {
     st = grow(ctx, ctx->ws.slist, cap2, k + 1, false);
     if (st != RZ_OK) return st;
     ctx->ws.list_cap = std::min(cap, cap2);
+    if (k <= kFastMaxK) return grow(ctx, ctx->ws.redlist, ctx->ws.red_cap, k + 1, false);
     return RZ_OK;
 }
 
@@ -73,6 +74,7 @@ int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.epoch, 0, 4, s));
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.arrive, 0, kMaxGrid * 4, s));
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.cnt_words, 0, 2 * kMaxGrid * 8, s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.arrive64, 0, kMaxGrid * 8, s));
     w.dirty = false;
     return RZ_OK;
 }
@@ -138,10 +140,11 @@ int rz_create(rz_ctx** out, int device) {
     Workspace& w = ctx->ws;
     void* p = nullptr;
     // One allocation: status | epoch | dev_len (one 256-byte line each) | arrival tags |
-    // tagged orphan counts | phase stamps.
+    // tagged orphan counts | tagged red-entry counts | phase stamps.
     const size_t off_arrive = 768;
     const size_t off_cnt = off_arrive + size_t(kMaxGrid) * 4;
-    const size_t off_stamps = off_cnt + size_t(2 * kMaxGrid) * 8;
+    const size_t off_arr64 = off_cnt + size_t(2 * kMaxGrid) * 8;
+    const size_t off_stamps = off_arr64 + size_t(kMaxGrid) * 8;
     const size_t bytes = off_stamps + size_t(kMaxGrid) * kStampsPerCta * 8;
     e = cudaMalloc(&p, bytes);
     if (e == cudaSuccess) e = cudaMemset(p, 0, bytes);
@@ -156,6 +159,7 @@ int rz_create(rz_ctx** out, int device) {
     w.dev_len = reinterpret_cast<unsigned long long*>(b + 512);
     w.arrive = reinterpret_cast<uint32_t*>(b + off_arrive);
     w.cnt_words = reinterpret_cast<unsigned long long*>(b + off_cnt);
+    w.arrive64 = reinterpret_cast<unsigned long long*>(b + off_arr64);
     w.stamps = reinterpret_cast<unsigned long long*>(b + off_stamps);
     *out = ctx;
     return RZ_OK;
@@ -170,6 +174,7 @@ void rz_destroy(rz_ctx* ctx) {
     cudaFree(w.bitmap);
     cudaFree(w.dlist);
     cudaFree(w.slist);
+    cudaFree(w.redlist);
     cudaFree(w.seen);
     cudaFree(w.part_bits);
     cudaFree(w.tile_state);

@@ -15,6 +15,11 @@ namespace rz {
 constexpr int kMaxGrid = 1024;           // upper bound on CTAs of the persistent single-list kernel
 constexpr int kStampsPerCta = 8;         // phase timestamps recorded per CTA when enabled
 constexpr uint32_t kSpinLimit = 1u << 22;  // polls of a bounded device wait (~0.5-1 s with backoff)
+// Red-list schedule of the grid kernel (one tile per CTA): every CTA publishes its red-zone
+// entries with its arrival, and when the whole grid has at most kFastMaxRed of them each CTA
+// derives the orphan pairing from that list in shared memory (no orphan-count exchange).
+constexpr uint32_t kFastMaxK = 1u << 17;   // k bound: two k-bit maps live in shared memory
+constexpr uint32_t kFastMaxRed = 1024;     // red entries of the whole grid
 
 // Library scratch owned by one context. Every buffer is zero where the kernels require it on
 // entry and is left zero on exit (the kernels clear what they set), so no per-call memset is
@@ -38,6 +43,9 @@ struct Workspace {
     uint32_t* epoch = nullptr;       // grid schedule: call epoch (advanced by CTA 0 each call)
     uint32_t* arrive = nullptr;      // grid schedule: per-CTA arrival tags, kMaxGrid
     unsigned long long* cnt_words = nullptr;  // grid schedule: tagged orphan counts, 2*kMaxGrid
+    unsigned long long* arrive64 = nullptr;   // red-list schedule: tag << 32 | red entries, kMaxGrid
+    uint2* redlist = nullptr;        // red-list schedule: {position, value - cut} per red entry, k
+    size_t red_cap = 0;
     unsigned long long* stamps = nullptr;     // optional phase timestamps, 8 per CTA
     bool stamps_on = false;
     bool dirty = false;
@@ -99,7 +107,7 @@ int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cu
 // Largest block size the single-list kernel for (w, items) can launch with.
 int redzone_max_block(int w, int items);
 // CTAs per SM the single-list kernel for (w, items, block) can keep resident.
-int redzone_occupancy(int w, int items, int block);
+int redzone_occupancy(int w, int items, int block, size_t dynamic_smem = 0);
 int default_cfg(const rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
 int clamp_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
 

@@ -156,6 +156,8 @@ extern "C" int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, c
     p.stamps = nullptr;
     p.spin_limit = kSpinLimit;
     p.validate = 0;
+    p.redlist = nullptr;  // bitmap schedule only: the fixed scratch array has no red list
+    p.arrive64 = nullptr;
 
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3(unsigned(grid));

@@ -15,6 +15,7 @@
 // Tiles are taken in ticket order, so every tile waited for is held by a running CTA that waits
 // for nothing before staging. The move kernel is one HBM pass (read n*w + n/8, write (n-k)*w).
 #include <algorithm>
+#include <atomic>
 #include <climits>
 
 #include "rz_common.cuh"
@@ -38,50 +39,98 @@ __global__ void partition_mark_kernel(const uint32_t* __restrict__ idx, uint32_t
     }
 }
 
-// Kept items of each tile (one warp per tile, grid-stride over tiles).
-__global__ void partition_count_kernel(const uint32_t* __restrict__ bits, uint32_t n, uint32_t tile_items,
-                                       uint32_t ntiles, uint32_t* __restrict__ kept) {
+// Kept items of each tile (one warp per tile, grid-stride over tiles). The bit map is padded with
+// zero words to whole tiles, so every tile's BW words are read as BW/4 16-byte loads, all issued
+// before any is used; only bits past n are masked.
+template <uint32_t BW>
+__global__ void partition_count_kernel(const uint32_t* __restrict__ bits, uint32_t n, uint32_t ntiles,
+                                       uint32_t* __restrict__ kept) {
+    constexpr uint32_t TILE = BW * 32u;
+    constexpr int V = int((BW / 4 + 31) / 32);  // 16-byte loads per lane
     const int lane = threadIdx.x & 31;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t wpt = tile_items >> 5;  // bitmap words per tile
     for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps) {
-        const uint32_t w0 = t * wpt;
+        const uint4* src = reinterpret_cast<const uint4*>(bits + size_t(t) * BW);
+        uint4 v[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            const uint32_t q = uint32_t(j) * 32u + uint32_t(lane);
+            v[j] = q < BW / 4 ? __ldg(&src[q]) : make_uint4(0u, 0u, 0u, 0u);
+        }
         uint32_t removed = 0;
-        for (uint32_t q = lane; q < wpt; q += 32) {
-            const uint32_t wi = w0 + q;
-            const uint32_t first = wi << 5;
-            if (first >= n) break;
-            uint32_t word = __ldg(&bits[wi]);
-            const uint32_t valid = n - first;
-            if (valid < 32) word &= (1u << valid) - 1u;  // bits past n are not items
-            removed += __popc(word);
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            const uint32_t q = uint32_t(j) * 32u + uint32_t(lane);
+            const uint32_t w[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t first = t * TILE + (q * 4u + uint32_t(e)) * 32u;
+                uint32_t word = w[e];
+                if (first >= n) word = 0u;
+                else if (n - first < 32u) word &= (1u << (n - first)) - 1u;  // bits past n are not items
+                removed += __popc(word);
+            }
         }
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) removed += __shfl_down_sync(0xffffffffu, removed, d);
-        if (lane == 0) {
-            const uint32_t items = min(tile_items, n - t * tile_items);
-            kept[t] = items - removed;
-        }
+        if (lane == 0) kept[t] = min(TILE, n - t * TILE) - removed;
     }
 }
 
 // Exclusive scan of kept[0..ntiles) into offset[0..ntiles) and the per-tile records
 // {offset, kept, 0, 0} the pipelined move copies with each tile; one CTA of 1024 threads.
+// Chunks of kScanChunk counts are loaded coalesced (all loads in flight at once) into shared
+// memory, each thread sums a contiguous run of 32, one block scan, and the results are written
+// back coalesced; a running carry joins the chunks.
+constexpr uint32_t kScanChunk = 32768;
+// One padding word per 32 keeps both the coalesced and the per-thread-run accesses free of bank
+// conflicts.
+__device__ __forceinline__ uint32_t scan_pad(uint32_t i) { return i + (i >> 5); }
+constexpr size_t kScanSmem = size_t(kScanChunk + kScanChunk / 32) * 4;
 __global__ void __launch_bounds__(1024) partition_scan_kernel(const uint32_t* __restrict__ kept, uint32_t ntiles,
                                                               uint32_t* __restrict__ offset, uint4* __restrict__ recs) {
+    extern __shared__ uint32_t s_kept[];  // [kScanChunk + kScanChunk / 32], padded
     __shared__ uint32_t scratch[33];
-    const uint32_t B = blockDim.x;
-    const uint32_t per = (ntiles + B - 1) / B;
-    const uint32_t lo = threadIdx.x * per, hi = min(lo + per, ntiles);
-    uint32_t s = 0;
-    for (uint32_t t = lo; t < hi; ++t) s += kept[t];
-    uint32_t total;
-    uint32_t run = block_exclusive_scan(s, scratch, &total);
-    for (uint32_t t = lo; t < hi; ++t) {
-        const uint32_t c = kept[t];
-        offset[t] = run;
-        recs[t] = make_uint4(run, c, 0u, 0u);
-        run += c;
+    constexpr uint32_t B = 1024, PER = kScanChunk / B;
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < ntiles; c0 += kScanChunk) {
+        const uint32_t cn = min(kScanChunk, ntiles - c0);
+        {
+            uint32_t v[PER];
+#pragma unroll
+            for (uint32_t j = 0; j < PER; ++j) {
+                const uint32_t q = j * B + threadIdx.x;
+                v[j] = q < cn ? kept[c0 + q] : 0u;
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < PER; ++j) s_kept[scan_pad(j * B + threadIdx.x)] = v[j];
+        }
+        __syncthreads();
+        uint32_t s = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < PER; ++j) s += s_kept[scan_pad(threadIdx.x * PER + j)];
+        uint32_t total;
+        uint32_t run = carry + block_exclusive_scan(s, scratch, &total);
+#pragma unroll
+        for (uint32_t j = 0; j < PER; ++j) {
+            const uint32_t x = s_kept[scan_pad(threadIdx.x * PER + j)];
+            s_kept[scan_pad(threadIdx.x * PER + j)] = run;
+            run += x;
+        }
+        __syncthreads();
+        const uint32_t end = carry + total;  // offset just past this chunk
+#pragma unroll 4
+        for (uint32_t j = 0; j < PER; ++j) {
+            const uint32_t q = j * B + threadIdx.x;
+            if (q < cn) {
+                const uint32_t o = s_kept[scan_pad(q)];
+                const uint32_t o_next = q + 1 < cn ? s_kept[scan_pad(q + 1)] : end;
+                offset[c0 + q] = o;
+                recs[c0 + q] = make_uint4(o, o_next - o, 0u, 0u);
+            }
+        }
+        carry = end;
+        __syncthreads();  // s_kept is reused by the next chunk
     }
 }
 
@@ -449,17 +498,30 @@ int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint
     const int mgrid = std::max(1, std::min<int>(ctx->sms * 8, int((k + 255) / 256)));
     partition_mark_kernel<<<mgrid, 256, 0, s>>>(idx, k, n, ctx->ws.part_bits, ctx->ws.status, validate ? 1u : 0u);
     const int cgrid = std::max(1, std::min<int>(ctx->sms * 8, int((ntiles + 7) / 8)));
-    partition_count_kernel<<<cgrid, 256, 0, s>>>(ctx->ws.part_bits, n, tile, ntiles, kept);
-    partition_scan_kernel<<<1, 1024, 0, s>>>(kept, ntiles, offset, recs);
+    switch (w) {
+        case 4: partition_count_kernel<kTileBytes / 4 / 32><<<cgrid, 256, 0, s>>>(ctx->ws.part_bits, n, ntiles, kept); break;
+        case 8: partition_count_kernel<kTileBytes / 8 / 32><<<cgrid, 256, 0, s>>>(ctx->ws.part_bits, n, ntiles, kept); break;
+        case 16: partition_count_kernel<kTileBytes / 16 / 32><<<cgrid, 256, 0, s>>>(ctx->ws.part_bits, n, ntiles, kept); break;
+        default: partition_count_kernel<kTileBytes / 32 / 32><<<cgrid, 256, 0, s>>>(ctx->ws.part_bits, n, ntiles, kept); break;
+    }
+    // Function attributes belong to a device: one bit per device (first 64 devices).
+    static std::atomic<uint64_t> scan_attr{0};
+    const uint64_t dev_bit = 1ull << (ctx->device & 63);
+    if (!(scan_attr.load() & dev_bit)) {
+        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)partition_scan_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, int(kScanSmem)));
+        scan_attr.fetch_or(dev_bit);
+    }
+    partition_scan_kernel<<<1, 1024, kScanSmem, s>>>(kept, ntiles, offset, recs);
     int grid = int(ntiles), block = kPartBlock;
     if ((reinterpret_cast<uintptr_t>(data) & 15u) == 0 && !ctx->ws.stamps_on) {
         size_t smem = 0;
         MoveWsFn f = move_ws_fn(int(w), &smem);
-        static bool attr_set[4] = {false, false, false, false};
+        static std::atomic<uint64_t> attr_set[4];
         const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
-        if (!attr_set[wi]) {
+        if (!(attr_set[wi].load() & dev_bit)) {
             RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-            attr_set[wi] = true;
+            attr_set[wi].fetch_or(dev_bit);
         }
         grid = std::max(1, std::min<int>(ctx->sms, int(ntiles)));
         block = kMoveBlock;

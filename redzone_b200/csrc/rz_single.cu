@@ -18,8 +18,17 @@
 //     epoch-tagged words; only CTAs that own destination orphans wait for the others, prefix the
 //     counts and binary-search the owner of each source rank (instead of the reference's
 //     LoadBalance linear search, :477-524).
+//   * Red-list schedule (one tile per CTA, k <= kFastMaxK): in phase A each CTA also writes its
+//     red entries {i, idx[i] - cut} in i order to its region of a list and arrives with a 64-bit
+//     word tag << 32 | count. If the grid holds at most kFastMaxRed red entries, every CTA reads
+//     them all into shared memory: V (tail positions whose item is removed) and P (positions whose
+//     hole needs no fill) as k-bit maps, destination orphans = V \ P counted per tile, source
+//     orphans = P \ V in order; each CTA then fills its holes and pairs its own destination
+//     orphans with no further exchange (phases B and C in one step, one grid-wide wait in all).
+//     Above that count the CTAs continue with the bitmap phases B and C.
 // The O(n) partition comparator is in rz_partition.cu; the cluster schedule in rz_cluster.cu.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "rz_common.cuh"
@@ -109,12 +118,25 @@ int redzone_max_block(int w, int items) {
     return c;
 }
 
-int redzone_occupancy(int w, int items, int block) {
+int redzone_occupancy(int w, int items, int block, size_t dynamic_smem) {
     SingleFn f = single_fn(w, items);
     if (!f) return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)f, block, 0) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)f, block, dynamic_smem) != cudaSuccess)
+        return 0;
     return nb;
+}
+
+// Opt the kernel in to the red-list schedule's dynamic shared memory (once per device and variant).
+static int allow_redlist_smem(rz_ctx* ctx, int w, int items) {
+    static std::atomic<uint64_t> done[4][4];
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    std::atomic<uint64_t>& d = done[wi(w)][ii(items)];
+    if (d.load() & bit) return RZ_OK;
+    RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)single_fn(w, items), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(redlist_smem_bytes(kFastMaxK))));
+    d.fetch_or(bit);
+    return RZ_OK;
 }
 
 int clamp_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg) {
@@ -189,16 +211,35 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     }
     const uint32_t tile = uint32_t(cfg.block) * uint32_t(cfg.items);
     const uint32_t ntiles = (k + tile - 1) / tile;
-    int occ = redzone_occupancy(int(w), cfg.items, cfg.block);
-    if (occ <= 0) return RZ_ERR_INVALID_ARG;
-    long grid = std::min<long>((long)cfg.ctas_per_sm, (long)occ) * ctx->sms;
-    grid = std::min<long>(grid, (long)ntiles);
-    grid = std::min<long>(grid, (long)kMaxGrid);
-    if (sched == RZ_SCHED_BLOCK) grid = 1;
-    if (grid < 1) grid = 1;
-    // Re-balance: use as many CTAs as needed for the resulting tiles-per-CTA (no idle CTAs).
-    const uint32_t tpc = (ntiles + uint32_t(grid) - 1) / uint32_t(grid);
-    grid = (ntiles + tpc - 1) / tpc;
+    // Red-list schedule when every tile gets its own co-resident CTA with the shared memory for
+    // the k-bit maps; otherwise the bitmap schedule without dynamic shared memory.
+    bool fast = false;
+    size_t dsmem = 0;
+    long grid = 1;
+    if (sched != RZ_SCHED_BLOCK && k <= kFastMaxK && ctx->ws.redlist && ntiles > 1) {
+        st = allow_redlist_smem(ctx, int(w), cfg.items);
+        if (st != RZ_OK) return st;
+        const size_t need = redlist_smem_bytes(k);
+        const int occf = redzone_occupancy(int(w), cfg.items, cfg.block, need);
+        const long gf = std::min<long>(std::min<long>((long)cfg.ctas_per_sm, (long)occf) * ctx->sms, (long)kMaxGrid);
+        if (occf > 0 && (long)ntiles <= gf) {
+            fast = true;
+            dsmem = need;
+            grid = ntiles;
+        }
+    }
+    if (!fast) {
+        int occ = redzone_occupancy(int(w), cfg.items, cfg.block);
+        if (occ <= 0) return RZ_ERR_INVALID_ARG;
+        grid = std::min<long>((long)cfg.ctas_per_sm, (long)occ) * ctx->sms;
+        grid = std::min<long>(grid, (long)ntiles);
+        grid = std::min<long>(grid, (long)kMaxGrid);
+        if (sched == RZ_SCHED_BLOCK) grid = 1;
+        if (grid < 1) grid = 1;
+        // Re-balance: use as many CTAs as needed for the resulting tiles-per-CTA (no idle CTAs).
+        const uint32_t tpc = (ntiles + uint32_t(grid) - 1) / uint32_t(grid);
+        grid = (ntiles + tpc - 1) / tpc;
+    }
 
     SingleParams p;
     p.data = static_cast<uint8_t*>(data);
@@ -216,12 +257,14 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     p.stamps = ctx->ws.stamps_on ? ctx->ws.stamps : nullptr;
     p.spin_limit = kSpinLimit;
     p.validate = validate ? 1u : 0u;
+    p.redlist = fast ? ctx->ws.redlist : nullptr;
+    p.arrive64 = fast ? ctx->ws.arrive64 : nullptr;
 
     SingleFn f = single_fn(int(w), cfg.items);
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3(unsigned(grid));
     lc.blockDim = dim3(unsigned(cfg.block));
-    lc.dynamicSmemBytes = 0;
+    lc.dynamicSmemBytes = dsmem;
     lc.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;

@@ -23,7 +23,34 @@ struct SingleParams {
     unsigned long long* stamps;  // nullable: 8 globaltimer stamps per CTA
     uint32_t spin_limit;
     uint32_t validate;
+    // Red-list schedule (nullable; set only with one tile per CTA, k <= kFastMaxK and the dynamic
+    // shared memory it needs): red entries per CTA region and tagged per-CTA entry counts.
+    uint2* redlist;
+    unsigned long long* arrive64;
 };
+
+// Exclusive scan in place of cbuf[0..E) by warp 0 (E <= 256, a few entries per lane); cbuf[E]
+// receives the total.
+__device__ __forceinline__ void warp0_scan_counts(uint32_t* cbuf, int E, int lane) {
+    const int per = (E + 31) >> 5;
+    const int lo = lane * per, hi = min(lo + per, E);
+    uint32_t s = 0;
+    for (int e = lo; e < hi; ++e) s += cbuf[e];
+    const uint32_t inc = warp_inclusive_scan(s);
+    uint32_t run = inc - s;
+    for (int e = lo; e < hi; ++e) {
+        const uint32_t x = cbuf[e];
+        cbuf[e] = run;
+        run += x;
+    }
+    if (lane == 31) cbuf[E] = inc;
+}
+
+// Dynamic shared memory of the red-list schedule for k removals: V and P maps (k bits each),
+// then red positions, red values and source orphans (kFastMaxRed words each).
+__host__ __device__ inline size_t redlist_smem_bytes(uint32_t k) {
+    return (size_t(2) * ((k + 31) / 32) + size_t(3) * kFastMaxRed) * 4;
+}
 
 // ------------------------------------------------------------------------------------------------
 // Redzone, one list, G persistent CTAs (G == 1 degenerates to block-level synchronisation).
@@ -51,6 +78,8 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     __shared__ uint32_t s_ps[kMaxGrid + 1];
     __shared__ int s_abort;
     __shared__ uint32_t s_tag;
+    extern __shared__ uint32_t s_dyn[];  // red-list schedule only
+    const bool fast = p.redlist != nullptr && single && G > 1;
 
     if (threadIdx.x == 0) {
         s_tag = (G > 1) ? ld_acquire(p.epoch) + 1u : 0u;
@@ -60,6 +89,8 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
 
     uint32_t rr[IPT];
     T src[IPT];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) rr[j] = 0xffffffffu;
 
     // ---- phase A: mark the red zone ---------------------------------------------------------
     // The loads are issued before the first __syncthreads so they overlap the epoch read.
@@ -105,10 +136,68 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     }
     RZ_STAMP(p, 1);
     const uint32_t tag = s_tag;
+    const int E = IPT * nw;
+
+    // ---- red-list schedule: publish this CTA's red entries {position, value - cut}, in position
+    // order, and clear the shared-memory maps used after the barrier.
+    uint32_t red_mine = 0;
+    if (fast) {
+        const uint32_t kw = (k + 31) >> 5;
+        for (uint32_t q = threadIdx.x; q < 2 * kw; q += B) s_dyn[q] = 0u;
+        uint32_t* cbuf = s_cnt[0];
+        uint32_t rm[IPT];
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+            const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
+            rm[j] = __ballot_sync(0xffffffffu, i < k && rr[j] >= cut && rr[j] < n);
+            if (lane == 0) cbuf[j * nw + warp] = __popc(rm[j]);
+        }
+        __syncthreads();
+        if (warp == 0) warp0_scan_counts(cbuf, E, lane);
+        __syncthreads();
+        const uint32_t lt = lanemask_lt();
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+            if ((rm[j] >> lane) & 1u) {
+                const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
+                p.redlist[chunk_base + cbuf[j * nw + warp] + __popc(rm[j] & lt)] = make_uint2(i, rr[j] - cut);
+            }
+        }
+        red_mine = cbuf[E];
+    }
+
     if (G > 1) {
-        flag_arrive(p.arrive, blockIdx.x, tag);
-        RZ_STAMP(p, 5);
-        if (!flag_wait_all(p.arrive, G, tag, p.status, p.spin_limit)) return;
+        if (fast) {
+            // Arrival carries the red-entry count: tag << 32 | count, released after the entries.
+            __syncthreads();
+            if (threadIdx.x == 0)
+                st_release_u64(&p.arrive64[blockIdx.x], ((unsigned long long)tag << 32) | red_mine);
+            RZ_STAMP(p, 5);
+            int ok = 1;
+            for (uint32_t c = threadIdx.x; c < G && ok; c += B) {
+                uint32_t it = 0;
+                unsigned long long w = ld_relaxed_u64(&p.arrive64[c]);
+                while (uint32_t(w >> 32) != tag) {
+                    if (++it > p.spin_limit) {
+                        ok = 0;
+                        break;
+                    }
+                    w = ld_relaxed_u64(&p.arrive64[c]);
+                }
+                s_pd[c] = uint32_t(w);
+            }
+            if (!__syncthreads_and(ok)) {
+                if (threadIdx.x == 0) atomicOr(p.status, ST_TIMEOUT);
+                return;
+            }
+            RZ_STAMP(p, 7);
+            if (threadIdx.x == 0) fence_acq_rel_gpu();  // the other CTAs' red entries and marks
+            __syncthreads();
+        } else {
+            flag_arrive(p.arrive, blockIdx.x, tag);
+            RZ_STAMP(p, 5);
+            if (!flag_wait_all(p.arrive, G, tag, p.status, p.spin_limit)) return;
+        }
         // Every CTA has read the epoch (it arrived): advance it for the next call.
         if (blockIdx.x == 0 && threadIdx.x == 0) *p.epoch = tag;
     } else {
@@ -116,11 +205,114 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     }
     RZ_STAMP(p, 2);
 
+    if (fast) {
+        block_scan_array(s_pd, int(G), s_scan);  // red entries before each CTA; s_pd[G] = total
+        if (s_pd[G] <= kFastMaxRed) {
+            // ---- every CTA derives the pairing from the red list -------------------------------
+            // V = tail positions i with cut + i in idx (sources that are removed), P = positions
+            // i with idx[i] >= cut (holes that need no filling). Destination orphans are V \ P
+            // and source orphans P \ V, both ranked in position order (the canonical rule).
+            const uint32_t R = s_pd[G];
+            const uint32_t kw = (k + 31) >> 5;
+            uint32_t* mapV = s_dyn;
+            uint32_t* mapP = s_dyn + kw;
+            uint32_t* s_pos = mapP + kw;
+            uint32_t* s_val = s_pos + kFastMaxRed;
+            uint32_t* s_src = s_val + kFastMaxRed;
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
+                if (i < k) src[j] = tail[i];  // L2 hit: prefetched in phase A
+            }
+            for (uint32_t e = threadIdx.x; e < R; e += B) {
+                const int c = owner_of_rank(s_pd, int(G), e);
+                const uint2 en = __ldcg(&p.redlist[size_t(c) * TILE + (e - s_pd[c])]);
+                s_pos[e] = en.x;
+                s_val[e] = en.y;
+                atomicOr(&mapV[en.y >> 5], 1u << (en.y & 31u));
+                atomicOr(&mapP[en.x >> 5], 1u << (en.x & 31u));
+            }
+            __syncthreads();
+            RZ_STAMP(p, 6);
+            // Ranks inside this tile: one word of the V \ P map per (round, warp).
+            uint32_t* cbuf = s_cnt[1];
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < IPT; ++j) {
+                    const uint32_t i0 = chunk_base + uint32_t(j) * B + uint32_t(warp) * 32u;
+                    cbuf[j * nw + warp] = i0 < k ? __popc(mapV[i0 >> 5] & ~mapP[i0 >> 5]) : 0u;
+                }
+            }
+            // Source orphans (P \ V) compacted in position order, destination orphans (V \ P)
+            // before this tile and in all: rounds of B red entries, per-warp ballot counts, one
+            // barrier per round (double-buffered counts; the first round always runs, so the
+            // tile's word counts above are published by it too).
+            const uint32_t lt = lanemask_lt();
+            uint32_t stot = 0, dbase = 0, dall = 0;
+            for (uint32_t q0 = 0, rd = 0; q0 == 0 || q0 < R; q0 += B, ++rd) {
+                uint32_t* wc = s_cnt[0] + 96u * (rd & 1u);
+                const uint32_t e = q0 + threadIdx.x;
+                uint32_t ps = 0;
+                bool sf = false, af = false, df = false;
+                if (e < R) {
+                    ps = s_pos[e];
+                    const uint32_t v = s_val[e];
+                    sf = !((mapV[ps >> 5] >> (ps & 31u)) & 1u);
+                    af = !((mapP[v >> 5] >> (v & 31u)) & 1u);
+                    df = af && v < chunk_base;
+                }
+                const uint32_t bs = __ballot_sync(0xffffffffu, sf);
+                const uint32_t bd = __ballot_sync(0xffffffffu, df);
+                const uint32_t ba = __ballot_sync(0xffffffffu, af);
+                if (lane == 0) {
+                    wc[warp] = __popc(bs);
+                    wc[32 + warp] = __popc(bd);
+                    wc[64 + warp] = __popc(ba);
+                }
+                __syncthreads();
+                uint32_t pre = 0, ts = 0;
+                for (int w2 = 0; w2 < nw; ++w2) {
+                    const uint32_t x = wc[w2];
+                    pre += w2 < warp ? x : 0u;
+                    ts += x;
+                    dbase += wc[32 + w2];
+                    dall += wc[64 + w2];
+                }
+                if (sf) s_src[stot + pre + __popc(bs & lt)] = ps;
+                stot += ts;
+            }
+            if (threadIdx.x == 0 && blockIdx.x == 0 && dall != stot) atomicOr(p.status, ST_INCONSISTENT);
+            if (warp == 0) warp0_scan_counts(cbuf, E, lane);
+            __syncthreads();  // s_src and the tile's ranks are complete
+            RZ_STAMP(p, 3);
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
+                if (i >= k || rr[j] >= cut) continue;  // past the list, or a hole needing no fill
+                const uint32_t vw = mapV[i >> 5];
+                if (!((vw >> lane) & 1u)) {
+                    head[rr[j]] = src[j];  // valid source, valid destination
+                } else {
+                    const uint32_t rank = dbase + cbuf[j * nw + warp] + __popc(vw & ~mapP[i >> 5] & lt);
+                    if (rank < stot) head[rr[j]] = tail[s_src[rank]];
+                }
+            }
+            if (lane == 0) {  // leave the global red-zone bitmap zero for the next call
+#pragma unroll
+                for (int j = 0; j < IPT; ++j) {
+                    const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
+                    if (i < k) p.bitmap[i >> 5] = 0u;
+                }
+            }
+            RZ_STAMP(p, 4);
+            return;
+        }
+    }
+
     // ---- phase B: classify, fill holes, collect orphans --------------------------------------
     // With one tile per CTA the hole writes are issued only after the orphan counts have been
     // published (below), so the publishing release does not wait for ~k scattered stores.
     uint32_t dcnt = 0, scnt = 0;
-    const int E = IPT * nw;
     bool dv[IPT], sv[IPT];
 #pragma unroll
     for (int j = 0; j < IPT; ++j) dv[j] = sv[j] = false;
@@ -177,20 +369,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
         }
         __syncthreads();
         if (tt == 0) RZ_STAMP(p, 6);
-        if (warp == 0) {
-            const int per = (E + 31) >> 5;
-            const int lo = lane * per, hi = min(lo + per, E);
-            uint32_t s = 0;
-            for (int e = lo; e < hi; ++e) s += cbuf[e];
-            const uint32_t inc = warp_inclusive_scan(s);
-            uint32_t run = inc - s;
-            for (int e = lo; e < hi; ++e) {
-                const uint32_t x = cbuf[e];
-                cbuf[e] = run;
-                run += x;
-            }
-            if (lane == 31) cbuf[E] = inc;
-        }
+        if (warp == 0) warp0_scan_counts(cbuf, E, lane);  // packed D << 16 | S counts
         __syncthreads();
         const uint32_t tot = cbuf[E];
         if (tot != 0u) {

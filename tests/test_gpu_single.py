@@ -190,6 +190,43 @@ def test_partition_many_tiles_per_cta(ctx):
         assert np.array_equal(got[: n - k], exp[: n - k]), (words, n, dist, k)
 
 
+@pytest.mark.parametrize("red", [0, 1, 2, 1023, 1024, 1025, 3000])
+@pytest.mark.parametrize("words", [1, 4])
+def test_red_list_schedule_around_its_limit(ctx, red, words):
+    """Exactly `red` indices in the red zone [n-k, n): up to 1024 of them the grid derives the
+    pairing from the published red list, above that it falls back to the bitmap exchange; the
+    results are the canonical ones either way (default and 256x4 launch configurations)."""
+    n, k = 1 << 20, 1 << 15
+    cut = n - k
+    rng = np.random.default_rng(red + 17 * words)
+    idx = np.concatenate([rng.choice(cut, size=k - red, replace=False),
+                          cut + rng.choice(k, size=red, replace=False)]).astype(np.uint32)
+    rng.shuffle(idx)
+    host = payload(n, words, seed=red)
+    exp = expect_of(host, idx)
+    for cfg in (None, rz.LaunchCfg(256, 4, 1, 0, 3), rz.LaunchCfg(128, 2, 4, 0, 3)):
+        got = run_gpu(ctx, host, idx, cfg=cfg)
+        assert np.array_equal(got[: n - k], exp[: n - k]), (red, words, cfg)
+
+
+def test_partition_more_tiles_than_one_scan_chunk(ctx):
+    """n = 2^28 + 3 tiles + 77 int32 items: 32,772 tiles of 8192, so the offset scan runs two
+    chunks with a carry; checked against a stable keep-mask compaction done by torch."""
+    n = (1 << 28) + 3 * 8192 + 77
+    k = 1 << 20
+    a = torch.arange(n, dtype=torch.int32, device=DEV)
+    g = torch.Generator(device=DEV)
+    g.manual_seed(7)
+    idx = torch.randperm(n, generator=g, device=DEV)[:k].to(torch.int32)
+    keep = torch.ones(n, dtype=torch.bool, device=DEV)
+    keep[idx.long()] = False
+    exp = a[keep]
+    ctx.partition(a, idx, flags=rz.RZ_SYNC)
+    assert torch.equal(a[: n - k], exp)
+    del a, exp, keep
+    torch.cuda.empty_cache()
+
+
 def test_append_then_remove(ctx):
     """Gains appended at the tail, then removal over the grown list (appended rows removable)."""
     for words, n, g, k in [(1, 1 << 18, 1 << 12, 1 << 13), (4, 5000, 300, 2000), (2, 1 << 16, 0, 100)]:
