@@ -155,16 +155,21 @@ int default_cfg(const rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch
     (void)n;
     cfg->use_partition = 0;
     cfg->schedule = RZ_SCHED_AUTO;
-    // Measured on B200 (n = 2^28 int32, L2 flushed): the 16-CTA cluster wins up to k = 2^14; above
-    // that the grid schedule with 512-thread CTAs, 1-2 items per thread up to 2^18, 4 beyond.
+    // Measured on B200 (n = 2^28, int32 and 16-byte items, L2 flushed, exhaustive autotune): the
+    // 16-CTA cluster wins up to k = 2^14; above that the grid schedule with 512-item tiles at 2^15,
+    // 1024-item tiles to 2^17 (64 CTAs at 2^16 -- fewer, fuller CTAs shorten the grid-wide wait),
+    // and 4096-item tiles on two CTAs per SM beyond.
     if (k <= kClusterMaxK) {
         cfg->block = 256; cfg->items = 4; cfg->ctas_per_sm = 4;
-    } else if (k <= (1u << 18)) {
-        cfg->block = 512; cfg->items = k <= (1u << 16) ? 1 : 2; cfg->ctas_per_sm = 4;
+    } else if (k <= (1u << 15)) {
+        cfg->block = 256; cfg->items = 2; cfg->ctas_per_sm = 4;
+    } else if (k <= (1u << 16)) {
+        cfg->block = 256; cfg->items = 4; cfg->ctas_per_sm = 2;
+    } else if (k <= (1u << 17)) {
+        cfg->block = 256; cfg->items = 4; cfg->ctas_per_sm = w >= 16 ? 2 : 1;
     } else {
-        cfg->block = 512; cfg->items = 4; cfg->ctas_per_sm = 4;
+        cfg->block = 1024; cfg->items = 4; cfg->ctas_per_sm = 2;
     }
-    if (w >= 16 && cfg->items > 2) cfg->items = 2;
     return clamp_cfg(ctx, k, w, cfg);
 }
 
