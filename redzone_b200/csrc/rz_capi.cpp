@@ -87,10 +87,22 @@ int map_status(uint32_t bits) {
     return RZ_OK;
 }
 
-int read_status(rz_ctx* ctx, cudaStream_t s) {
+// The status word (offset 0) and the device length (offset 512) of the workspace block come back
+// in one copy on the call's stream into pinned memory, then one stream synchronisation.
+static constexpr size_t kResultBytes = 512 + sizeof(unsigned long long);
+
+static int fetch_result(rz_ctx* ctx, cudaStream_t s, uint32_t* status, unsigned long long* len) {
+    RZ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ws.h_result, ctx->ws.status, kResultBytes, cudaMemcpyDeviceToHost, s));
     RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    std::memcpy(status, ctx->ws.h_result, sizeof(uint32_t));
+    if (len) std::memcpy(len, ctx->ws.h_result + 512, sizeof(unsigned long long));
+    return RZ_OK;
+}
+
+int read_status(rz_ctx* ctx, cudaStream_t s) {
     uint32_t h = 0;
-    RZ_CUDA_TRY(ctx, cudaMemcpy(&h, ctx->ws.status, sizeof(h), cudaMemcpyDeviceToHost));
+    int st = fetch_result(ctx, s, &h, nullptr);
+    if (st != RZ_OK) return st;
     if (h) {
         RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
         // A failed call may have left barrier state or bitmap bits behind.
@@ -161,6 +173,15 @@ int rz_create(rz_ctx** out, int device) {
     w.cnt_words = reinterpret_cast<unsigned long long*>(b + off_cnt);
     w.arrive64 = reinterpret_cast<unsigned long long*>(b + off_arr64);
     w.stamps = reinterpret_cast<unsigned long long*>(b + off_stamps);
+    void* hr = nullptr;
+    e = cudaMallocHost(&hr, kResultBytes);
+    if (e != cudaSuccess) {
+        int st = cuda_fail(ctx, e, "pinned result buffer");
+        cudaFree(p);
+        delete ctx;
+        return st;
+    }
+    w.h_result = static_cast<uint8_t*>(hr);
     *out = ctx;
     return RZ_OK;
 }
@@ -171,6 +192,7 @@ void rz_destroy(rz_ctx* ctx) {
     cudaDeviceSynchronize();
     Workspace& w = ctx->ws;
     cudaFree(w.status);
+    if (w.h_result) cudaFreeHost(w.h_result);
     cudaFree(w.bitmap);
     cudaFree(w.dlist);
     cudaFree(w.slist);
@@ -319,14 +341,17 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
     int64_t nl = 0;
     st = rz_remove(ctx, d_data, n, elem_bytes, d_stage, k, &nl, flags & ~RZ_SYNC, stream);
     if (st != RZ_OK) return st;
-    // Read the device-tracked length back: the step's result crosses to the host.
+    // Read the device-tracked length back with the status: the step's result crosses to the host.
     unsigned long long dl = 0;
-    if (k > 0 && k < n) {
-        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(&dl, ctx->ws.dev_len, sizeof(dl), cudaMemcpyDeviceToHost, s));
+    uint32_t h = 0;
+    st = fetch_result(ctx, s, &h, &dl);
+    if (st != RZ_OK) return st;
+    if (h) {
+        RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
+        ctx->ws.dirty = true;
     }
-    st = read_status(ctx, s);
     if (new_len) *new_len = (k > 0 && k < n) ? int64_t(dl) : n - k;
-    return st;
+    return map_status(h);
 }
 
 int rz_last_launch(const rz_ctx* ctx, int32_t* kernels, int32_t* grid, int32_t* block) {

@@ -47,6 +47,7 @@ struct Workspace {
     uint2* redlist = nullptr;        // red-list schedule: {position, value - cut} per red entry, k
     size_t red_cap = 0;
     unsigned long long* stamps = nullptr;     // optional phase timestamps, 8 per CTA
+    uint8_t* h_result = nullptr;     // pinned host copy of [status .. dev_len] (one D2H per sync)
     bool stamps_on = false;
     bool dirty = false;
 };
