@@ -160,6 +160,7 @@ __global__ void redzone_batched_kernel(const BatchParams p) {
         if (kind == K_MARK) {
             for (uint32_t c = t_begin; c < t_end; ++c) {
                 const uint32_t base = c * TILE;
+                if (c + 1 < t_end) prefetch_l2(L.idx + base + TILE, size_t(min(TILE, k - base - TILE)) * 4);
 #pragma unroll
                 for (int j = 0; j < IPT; ++j) {
                     const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
@@ -190,7 +191,11 @@ __global__ void redzone_batched_kernel(const BatchParams p) {
 #pragma unroll
             for (int j = 0; j < IPT; ++j) {
                 const uint32_t i = uint32_t(j) * B + threadIdx.x;
-                rr[j] = (i < k) ? __ldg(&L.idx[i]) : 0xffffffffu;
+                rr[j] = 0xffffffffu;
+                if (i < k) {
+                    rr[j] = __ldg(&L.idx[i]);
+                    src[j] = tail[i];  // loaded with the index, needed or not: one round trip
+                }
             }
             for (uint32_t w = threadIdx.x; w < TILE / 32; w += B) s_bits[w] = 0u;
             __syncthreads();
@@ -209,7 +214,6 @@ __global__ void redzone_batched_kernel(const BatchParams p) {
                 if (i < k) {
                     sv[j] = ((s_bits[i >> 5] >> (i & 31u)) & 1u) == 0u;
                     dv[j] = rr[j] < cut;
-                    if (dv[j] && sv[j]) src[j] = tail[i];
                 } else {
                     sv[j] = dv[j] = false;
                 }
@@ -240,19 +244,33 @@ __global__ void redzone_batched_kernel(const BatchParams p) {
             }
             for (uint32_t c = t_begin; c < t_end; ++c) {
                 const uint32_t base = c * TILE;
+                // The next tile's indices and tail window go to L2 while this one is processed.
+                if (c + 1 < t_end) {
+                    const uint32_t nb = base + TILE, cnt = min(TILE, k - nb);
+                    prefetch_l2(L.idx + nb, size_t(cnt) * 4);
+                    prefetch_l2(tail + nb, size_t(cnt) * W);
+                }
+                // Index, bitmap word and tail item are loaded together (the tail item whether it
+                // is needed or not): one round trip per tile instead of two dependent ones.
+                uint32_t word[IPT];
 #pragma unroll
                 for (int j = 0; j < IPT; ++j) {
                     const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-                    rr[j] = (i < k) ? __ldg(&L.idx[i]) : 0xffffffffu;
+                    if (i < k) {
+                        rr[j] = __ldg(&L.idx[i]);
+                        word[j] = __ldcg(&p.bitmap[L.bitmap_off + (i >> 5)]);
+                        src[j] = tail[i];
+                    } else {
+                        rr[j] = 0xffffffffu;
+                        word[j] = 0u;
+                    }
                 }
 #pragma unroll
                 for (int j = 0; j < IPT; ++j) {
                     const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
                     if (i < k) {
-                        const uint32_t word = __ldcg(&p.bitmap[L.bitmap_off + (i >> 5)]);
-                        sv[j] = ((word >> (i & 31u)) & 1u) == 0u;
+                        sv[j] = ((word[j] >> (i & 31u)) & 1u) == 0u;
                         dv[j] = rr[j] < cut;
-                        if (dv[j] && sv[j]) src[j] = tail[i];
                     } else {
                         sv[j] = dv[j] = false;
                     }

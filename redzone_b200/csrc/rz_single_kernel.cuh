@@ -106,6 +106,8 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
             // is not an outstanding access the arrival's release has to wait for (a load is).
             const uint32_t cnt = min(TILE, k - base);
             prefetch_l2(tail + base, size_t(cnt) * W);
+        } else if (t + 1 < t1) {
+            prefetch_l2(p.idx + base + TILE, size_t(min(TILE, k - base - TILE)) * 4);  // next tile
         }
         if (t == t0) {
             __syncthreads();  // s_abort / s_tag
@@ -318,20 +320,32 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     for (int j = 0; j < IPT; ++j) dv[j] = sv[j] = false;
     for (uint32_t t = t0, tt = 0; t < t1; ++t, ++tt) {
         const uint32_t base = t * TILE;
-        if (!single) {
+        if (!single && t + 1 < t1) {
+            // The next tile's indices and tail window go to L2 while this one is processed.
+            const uint32_t nb = base + TILE, cnt = min(TILE, k - nb);
+            prefetch_l2(p.idx + nb, size_t(cnt) * 4);
+            prefetch_l2(tail + nb, size_t(cnt) * W);
+        }
+        // Index (re-read when a CTA has several tiles), bitmap word and tail item are loaded
+        // together, the tail item whether it is needed or not: one round trip per tile.
+        uint32_t word[IPT];
 #pragma unroll
-            for (int j = 0; j < IPT; ++j) {
-                const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-                rr[j] = (i < k) ? __ldg(&p.idx[i]) : 0xffffffffu;
+        for (int j = 0; j < IPT; ++j) {
+            const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
+            if (i < k) {
+                if (!single) rr[j] = __ldg(&p.idx[i]);
+                word[j] = __ldcg(&p.bitmap[i >> 5]);
+                src[j] = tail[i];  // with one tile per CTA: an L2 hit (prefetched in phase A)
+            } else {
+                if (!single) rr[j] = 0xffffffffu;
+                word[j] = 0u;
             }
         }
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
             if (i < k) {
-                const uint32_t word = __ldcg(&p.bitmap[i >> 5]);
-                if (single) src[j] = tail[i];  // L2 hit (prefetched), issued with the bitmap load
-                sv[j] = ((word >> (i & 31u)) & 1u) == 0u;
+                sv[j] = ((word[j] >> (i & 31u)) & 1u) == 0u;
                 dv[j] = rr[j] < cut;
             } else {
                 sv[j] = false;
@@ -339,11 +353,6 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
             }
         }
         if (!single) {
-#pragma unroll
-            for (int j = 0; j < IPT; ++j) {
-                const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-                if (dv[j] && sv[j]) src[j] = tail[i];
-            }
 #pragma unroll
             for (int j = 0; j < IPT; ++j)
                 if (dv[j] && sv[j]) head[rr[j]] = src[j];
