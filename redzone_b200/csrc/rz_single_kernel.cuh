@@ -78,6 +78,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     __shared__ uint32_t s_ps[kMaxGrid + 1];
     __shared__ int s_abort;
     __shared__ uint32_t s_tag;
+    __shared__ uint32_t s_red_total;     // red-list schedule: red entries of the whole grid
     extern __shared__ uint32_t s_dyn[];  // red-list schedule only
     const bool fast = p.redlist != nullptr && single && G > 1;
 
@@ -146,6 +147,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     if (fast) {
         const uint32_t kw = (k + 31) >> 5;
         for (uint32_t q = threadIdx.x; q < 2 * kw; q += B) s_dyn[q] = 0u;
+        if (threadIdx.x == 0) s_red_total = 0u;
         uint32_t* cbuf = s_cnt[0];
         uint32_t rm[IPT];
 #pragma unroll
@@ -187,6 +189,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
                     w = ld_relaxed_u64(&p.arrive64[c]);
                 }
                 s_pd[c] = uint32_t(w);
+                atomicAdd(&s_red_total, uint32_t(w));
             }
             if (!__syncthreads_and(ok)) {
                 if (threadIdx.x == 0) atomicOr(p.status, ST_TIMEOUT);
@@ -208,31 +211,48 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
     RZ_STAMP(p, 2);
 
     if (fast) {
-        block_scan_array(s_pd, int(G), s_scan);  // red entries before each CTA; s_pd[G] = total
-        if (s_pd[G] <= kFastMaxRed) {
+        if (s_red_total <= kFastMaxRed) {
             // ---- every CTA derives the pairing from the red list -------------------------------
             // V = tail positions i with cut + i in idx (sources that are removed), P = positions
             // i with idx[i] >= cut (holes that need no filling). Destination orphans are V \ P
             // and source orphans P \ V, both ranked in position order (the canonical rule).
-            const uint32_t R = s_pd[G];
+            const uint32_t R = s_red_total;
             const uint32_t kw = (k + 31) >> 5;
             uint32_t* mapV = s_dyn;
             uint32_t* mapP = s_dyn + kw;
-            uint32_t* s_pos = mapP + kw;
+            uint32_t* s_pos = mapP + kw;  // red positions, in position order
             uint32_t* s_val = s_pos + kFastMaxRed;
-            uint32_t* s_src = s_val + kFastMaxRed;
+            uint32_t* s_src = s_val + kFastMaxRed;  // source orphans, in position order
 #pragma unroll
             for (int j = 0; j < IPT; ++j) {
                 const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
                 if (i < k) src[j] = tail[i];  // L2 hit: prefetched in phase A
             }
-            for (uint32_t e = threadIdx.x; e < R; e += B) {
-                const int c = owner_of_rank(s_pd, int(G), e);
-                const uint2 en = __ldcg(&p.redlist[size_t(c) * TILE + (e - s_pd[c])]);
-                s_pos[e] = en.x;
-                s_val[e] = en.y;
-                atomicOr(&mapV[en.y >> 5], 1u << (en.y & 31u));
-                atomicOr(&mapP[en.x >> 5], 1u << (en.x & 31u));
+            // Red entries before each CTA: warp 0 scans the G counts (a few per lane, in order).
+            if (warp == 0) {
+                const uint32_t per = (G + 31) >> 5;
+                const uint32_t ca = min(uint32_t(lane) * per, G), cb = min(ca + per, G);
+                uint32_t s = 0;
+                for (uint32_t c = ca; c < cb; ++c) s += s_pd[c];
+                uint32_t run = warp_inclusive_scan(s) - s;
+                for (uint32_t c = ca; c < cb; ++c) {
+                    const uint32_t x = s_pd[c];
+                    s_ps[c] = run;  // exclusive prefix; s_pd keeps the counts
+                    run += x;
+                }
+            }
+            __syncthreads();
+            // Gather, in position order: thread c copies CTA c's entries to their ranks.
+            for (uint32_t c = threadIdx.x; c < G; c += B) {
+                const uint32_t cnt = s_pd[c], at = s_ps[c];
+                const uint2* ent = p.redlist + size_t(c) * TILE;
+                for (uint32_t e = 0; e < cnt; ++e) {
+                    const uint2 en = __ldcg(&ent[e]);
+                    s_pos[at + e] = en.x;
+                    s_val[at + e] = en.y;
+                    atomicOr(&mapV[en.y >> 5], 1u << (en.y & 31u));
+                    atomicOr(&mapP[en.x >> 5], 1u << (en.x & 31u));
+                }
             }
             __syncthreads();
             RZ_STAMP(p, 6);
