@@ -120,10 +120,8 @@ class ClockSampler:
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from redzone_b200 import dist
+    return dist.env_ranks()
 
 
 def alg_bytes(n: int, k: int, w: int, idx: np.ndarray) -> float:
@@ -195,14 +193,10 @@ def reference_arm(args):
 def own_arm(args):
     import torch
 
-    world, rank, local = dist_init(args)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    else:
+    from redzone_b200 import dist
+
+    world, rank, local = dist.init("nccl")
+    if world == 1:
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
     import redzone_b200 as rz
@@ -212,7 +206,7 @@ def own_arm(args):
     ctx = rz.Context(dev.index)
     n, k = 1 << N_LOG2, 1 << K_LOG2
     a = torch.arange(n, dtype=torch.int32, device=dev)
-    sets_np = [workloads.uniform(n, k, seed=1000 * rank + s) for s in range(NSETS)]
+    sets_np = [workloads.uniform(n, k, seed=dist.replica_seed(s, rank)) for s in range(NSETS)]
     sets = [torch.from_numpy(s.astype(np.int32)).to(dev) for s in sets_np]
     pinned = [torch.from_numpy(s.astype(np.int32)).pin_memory() for s in sets_np]
     scrub = torch.empty(SCRUB_BYTES, dtype=torch.uint8, device=dev)
@@ -226,16 +220,10 @@ def own_arm(args):
     kernels_per_call, grid, block = ctx.last_launch()
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
+        dist.barrier(dev)
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return dist.max_over_ranks(x, dev)
 
     # ---- Redzone, device-resident inputs ----
     for i in range(args.warmup):

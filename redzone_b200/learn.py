@@ -142,12 +142,13 @@ def soft_targets(times: np.ndarray, tau: float = 0.03) -> np.ndarray:
 
 def draw_instance(rng: np.random.Generator) -> tuple[int, int, int, str]:
     """(n, k, w, distribution): mixes of the n = 2^20 (k = 2^14) and n = 2^28 (k sweep, int32 and
-    16-byte items) configurations, with intermediate list sizes for coverage."""
+    16-byte items) configurations, with intermediate list sizes for coverage. k reaches 2^24, where
+    the O(n) partition overtakes the O(k) removal at n = 2^28."""
     if rng.random() < 0.15:
         n, k = 1 << 20, 1 << 14
     else:
         n = 1 << int(rng.choice([16, 18, 20, 22, 24, 26, 28], p=[.08, .1, .14, .14, .16, .14, .24]))
-        hi = math.log2(n) - 1 if n <= (1 << 24) else 22.0
+        hi = min(math.log2(n) - 1, 24.0)
         k = int(round(2 ** rng.uniform(8.0, hi)))
     w = int(rng.choice([4, 16]))
     dist = str(rng.choice(["uniform", "clustered", "tail"], p=[.6, .2, .2]))
