@@ -405,23 +405,30 @@ def batched(args):
     launch per list (stream-launched, and the same launches captured in one CUDA graph)."""
     import torch
     import redzone_b200 as rz
-    from redzone_b200 import _native, workloads
+    from redzone_b200 import _native, dist, workloads
 
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
-    ctx = rz.Context(0)
-    nlists = args.lists
-    n, k = workloads.batched_lists(nlists, seed=args.seed)
-    total_n, total_k = int(n.sum()), int(k.sum())
-    buf = torch.empty(total_n, dtype=torch.int64, device=dev)
+    # N > 1: the lists are partitioned across ranks by removals (contiguous, balanced), each rank
+    # runs its share as one launch; no collective on the data path, max-over-ranks timing.
+    world, rank, local = dist.init("nccl")
+    if world == 1:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctx = rz.Context(dev.index)
+    nlists_all = args.lists
+    n_all, k_all = workloads.batched_lists(nlists_all, seed=args.seed)
+    total_n, total_k = int(n_all.sum()), int(k_all.sum())
+    mine = dist.shard_by_weight(k_all, world, rank)
+    nlists = len(mine)
+    n, k = n_all[mine], k_all[mine]
+    buf = torch.empty(int(n.sum()), dtype=torch.int64, device=dev)
     g = torch.Generator(device=dev)
-    g.manual_seed(args.seed)
     lists, off = [], 0
-    for l in range(nlists):
-        ni, ki = int(n[l]), int(k[l])
+    for q, l in enumerate(mine):
+        ni, ki = int(n[q]), int(k[q])
         seg = buf[off: off + ni]
         torch.arange(ni, out=seg)
-        seg.add_(l << 32)
+        seg.add_(int(l) << 32)
+        g.manual_seed(args.seed * 100003 + int(l))  # the list's indices depend on the list alone
         idx = torch.randperm(ni, generator=g, device=dev)[:ki].to(torch.int32)
         lists.append((seg, idx))
         off += ni
@@ -463,35 +470,39 @@ def batched(args):
 
     for _ in range(args.warmup):
         plan.launch()
-    batched_ms = timed(plan.launch, args.steps)
+    dist.barrier(dev)
+    batched_ms = dist.max_over_ranks(timed(plan.launch, args.steps), dev)
 
     def plain():
         for d, i in lists:
             ctx.remove(d, i)
     plain()
-    plain_ms = timed(plain, max(3, args.steps // 5))
+    plain_ms = dist.max_over_ranks(timed(plain, max(3, args.steps // 5)), dev)
     # The same per-list launches captured once into a CUDA graph (no host launch overhead).
     plain_graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(plain_graph):
         plain()
     plain_graph.replay()
-    plain_graph_ms = timed(plain_graph.replay, max(3, args.steps // 5))
+    plain_graph_ms = dist.max_over_ranks(timed(plain_graph.replay, max(3, args.steps // 5)), dev)
     del plain_graph
     info = plan.info()
     w = 8
-    k_r = 0  # algorithmic bytes: red-zone entries per list
+    # Algorithmic bytes: red-zone entries estimated from a sample of this rank's lists.
+    kr_s = k_s = 0
     for d, i in lists[:: max(1, nlists // 256)]:
-        k_r += int((i >= d.shape[0] - i.numel()).sum().item())
-    k_r = k_r * max(1, nlists // 256)
+        kr_s += int((i >= d.shape[0] - i.numel()).sum().item())
+        k_s += i.numel()
+    k_r = total_k * (kr_s / max(1, k_s))
     balg = 4.0 * total_k + 2.0 * w * (total_k - k_r) + total_k / 4.0
     peak, peak_kind = load_peaks()
     line = {
-        "metric": METRIC, "value": total_k / (batched_ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"{nlists} lists, n log-uniform [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), "
-                               f"uint64 payload (list id << 32 | index), one persistent graph-replayed launch",
+        "metric": METRIC, "value": total_k / (batched_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"{nlists_all} lists, n log-uniform [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), "
+                               f"uint64 payload (list id << 32 | index), one persistent graph-replayed launch per GPU",
                    "total_n": total_n, "total_k": total_k, "batch_cfg": info,
+                   "parallelism": "single GPU" if world == 1 else f"{world} GPUs, lists partitioned by removals",
                    "tuned_ms": float(best_ms.value) if cfg is not None else None},
         "plain_per_list": {"ms_per_step": plain_ms, "speedup_batched_vs_plain": plain_ms / batched_ms},
         "plain_per_list_graph": {"ms_per_step": plain_graph_ms, "speedup_batched_vs_plain": plain_graph_ms / batched_ms},
@@ -499,9 +510,14 @@ def batched(args):
                      "frac": balg / (batched_ms * 1e-3) / 1e9 / peak, "traffic": None, "alg_bytes_per_launch": balg},
         "gpu_launches": args.steps,
     }
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
 
 
 def service(args):
