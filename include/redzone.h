@@ -123,6 +123,17 @@ int rz_append_remove(rz_ctx* ctx, void* d_data, int64_t n, int64_t capacity, uin
                      uint32_t flags, rz_stream_t stream);
 
 /*
+ * Preserve-list compaction, the inverse form of removal: d_data[0..m) = (old) d_data[d_keep[j]]
+ * for j in [0, m), in the order of d_keep (any order; each entry < n). O(m) work -- cheaper than
+ * removing the other n - m items when m < n/2. The kept items pass through context scratch
+ * (m * elem_bytes, grown on first use). Entries >= n are skipped and reported as
+ * RZ_ERR_OUT_OF_RANGE (with RZ_SYNC or rz_sync_status). *new_len = m. No counterpart in the
+ * reference's code (the paper names it as future work).
+ */
+int rz_keep(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_keep, int64_t m,
+            int64_t* new_len, uint32_t flags, rz_stream_t stream);
+
+/*
  * O(n) stable partition comparator (mark, per-tile counts and their scan, then a pipelined
  * in-place move), in place. Survivors keep their relative order, as with thrust::remove
  * (Thrust_remove.hxx:15-17) and InK compact (cuCompactor.cuh:104-141).

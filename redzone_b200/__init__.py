@@ -109,6 +109,16 @@ class Context:
         self._check(st, "rz_append_remove")
         return out.value
 
+    def keep(self, data, keep, flags: int = 0, stream=None) -> int:
+        """Preserve-list compaction: data[0..m) = (old) data[keep[j]], O(m); returns m."""
+        n, m = int(data.shape[0]), int(keep.numel())
+        out = ctypes.c_int64(0)
+        st = _native.lib.rz_keep(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
+                                 ctypes.c_void_p(keep.data_ptr()), m, ctypes.byref(out), flags,
+                                 ctypes.c_void_p(_stream_handle(stream)))
+        self._check(st, "rz_keep")
+        return out.value
+
     def partition(self, data, idx, flags: int = 0, stream=None) -> int:
         """O(n) stable partition comparator (survivors keep their order)."""
         n, k = int(data.shape[0]), int(idx.numel())

@@ -201,6 +201,7 @@ void rz_destroy(rz_ctx* ctx) {
     cudaFree(w.part_bits);
     cudaFree(w.tile_state);
     cudaFree(w.idx_stage);
+    cudaFree(w.keep_stage);
     release_extras(ctx);
     delete ctx;
 }
@@ -314,6 +315,26 @@ int rz_append_remove(rz_ctx* ctx, void* d_data, int64_t n, int64_t capacity, uin
                                          reinterpret_cast<cudaStream_t>(stream)));
     }
     return rz_remove(ctx, d_data, n + g, elem_bytes, d_idx, k, new_len, flags, stream);
+}
+
+int rz_keep(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_keep, int64_t m,
+            int64_t* new_len, uint32_t flags, rz_stream_t stream) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    // The keep list may be any length up to n and in any order: the same checks as a removal
+    // list of the same length.
+    int st = check_args(d_data, n, elem_bytes, d_keep, m);
+    if (st != RZ_OK) return st;
+    if (new_len) *new_len = m;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    st = grow(ctx, ctx->ws.keep_stage, ctx->ws.keep_cap, (size_t(m) * elem_bytes + 15) / 16 + 1, false);
+    if (st != RZ_OK) return st;
+    st = launch_keep(ctx, d_data, uint32_t(n), elem_bytes, d_keep, uint32_t(m), ctx->ws.keep_stage, s);
+    if (st != RZ_OK) return st;
+    ctx->last_kernels = m > 0 ? 1 : 0;
+    if (flags & RZ_SYNC) return read_status(ctx, s);
+    return RZ_OK;
 }
 
 int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,

@@ -40,6 +40,8 @@ struct Workspace {
     unsigned long long* dev_len = nullptr;     // device copy of the last new length
     uint32_t* idx_stage = nullptr;   // rz_remove_host_idx: device copy of host indices
     size_t stage_cap = 0;
+    uint4* keep_stage = nullptr;     // rz_keep: the kept items, 16-byte units
+    size_t keep_cap = 0;
     uint32_t* epoch = nullptr;       // grid schedule: call epoch (advanced by CTA 0 each call)
     uint32_t* arrive = nullptr;      // grid schedule: per-CTA arrival tags, kMaxGrid
     unsigned long long* cnt_words = nullptr;  // grid schedule: tagged orphan counts, 2*kMaxGrid
@@ -105,6 +107,9 @@ constexpr uint32_t kClusterMaxK = 1u << 14;  // RZ_SCHED_AUTO uses the cluster s
 // The 48-point launch-configuration space in its canonical order (rz_autotune.cpp).
 void config_space(rz_launch_cfg* out48);
 int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cudaStream_t s);
+// rz_keep: gather data[keep[j]] into `stage` (m items), then copy the stage to data[0..m).
+int launch_keep(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* keep, uint32_t m, void* stage,
+                cudaStream_t s);
 // Largest block size the single-list kernel for (w, items) can launch with.
 int redzone_max_block(int w, int items);
 // CTAs per SM the single-list kernel for (w, items, block) can keep resident.

@@ -227,6 +227,35 @@ def test_partition_more_tiles_than_one_scan_chunk(ctx):
     torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("words", [1, 2, 4, 8])
+def test_preserve_list_compaction(ctx, words):
+    """rz_keep: data[0..m) = old data[keep[j]] for sorted, unsorted, empty and full keep lists
+    (reads from [0, m) included); the rest of the array is untouched; an entry >= n is skipped
+    and reported."""
+    rng = np.random.default_rng(words)
+    n = (1 << 18) + 13
+    for m, order in [(0, "sorted"), (1, "sorted"), (1000, "sorted"), (1 << 16, "random"), (n // 2, "sorted"),
+                     (n, "random")]:
+        host = payload(n, words, seed=m + words)
+        keep = rng.choice(n, size=m, replace=False).astype(np.uint32)
+        if order == "sorted":
+            keep.sort()
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        new_len = ctx.keep(d, torch.from_numpy(keep.view(np.int32)).to(DEV), flags=rz.RZ_SYNC)
+        assert new_len == m
+        got = d.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got[:m], host[keep]), (words, m, order)
+        assert np.array_equal(got[m:], host[m:])
+    keep = np.array([5, n + 7, 9], dtype=np.uint32)
+    host = payload(n, words, seed=1)
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.keep(d, torch.from_numpy(keep.view(np.int32)).to(DEV), flags=rz.RZ_SYNC)
+    assert e.value.code == 3
+    got = d.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got[0], host[5]) and np.array_equal(got[1], host[1]) and np.array_equal(got[2], host[9])
+
+
 def test_append_then_remove(ctx):
     """Gains appended at the tail, then removal over the grown list (appended rows removable)."""
     for words, n, g, k in [(1, 1 << 18, 1 << 12, 1 << 13), (4, 5000, 300, 2000), (2, 1 << 16, 0, 100)]:
