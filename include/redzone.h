@@ -134,6 +134,31 @@ int rz_keep(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uin
             int64_t* new_len, uint32_t flags, rz_stream_t stream);
 
 /*
+ * Key -> row index for delete-by-key (no counterpart in the reference's code; the paper names a
+ * key index kept under Redzone moves as future work). Records are 8, 16 or 32 bytes and begin
+ * with a uint64 key; the two largest key values are reserved. The index is a device hash table of
+ * `capacity` slots (rounded up to a power of two; keep it at least twice the live keys).
+ *   rz_keyindex_build  -- clear, then index rows [0, n); RZ_ERR_DUPLICATE on a repeated key.
+ *   rz_keyindex_insert -- index rows [first, first + count) (e.g. after rz_append_remove); the
+ *                         keys must not be indexed already. Both are synchronous.
+ *   rz_keyindex_find   -- rows of `count` keys into d_rows (0xffffffff when absent), async.
+ *   rz_remove_by_key   -- remove the rows holding the k given keys with the Redzone rule and keep
+ *                         the index exact: deleted keys are erased and each item moved into a hole
+ *                         is re-pointed at it (O(k); no other row changes). Synchronous up to the
+ *                         removal: a missing key returns RZ_ERR_OUT_OF_RANGE and a repeated one
+ *                         RZ_ERR_DUPLICATE before any row moves. *new_len = n - k.
+ */
+typedef struct rz_keyindex rz_keyindex;
+int rz_keyindex_create(rz_ctx* ctx, int64_t capacity, rz_keyindex** out);
+void rz_keyindex_destroy(rz_keyindex* ix);
+int rz_keyindex_build(rz_keyindex* ix, const void* d_data, int64_t n, uint32_t record_bytes, rz_stream_t stream);
+int rz_keyindex_insert(rz_keyindex* ix, const void* d_data, int64_t first, int64_t count, uint32_t record_bytes,
+                       rz_stream_t stream);
+int rz_keyindex_find(rz_keyindex* ix, const uint64_t* d_keys, int64_t count, uint32_t* d_rows, rz_stream_t stream);
+int rz_remove_by_key(rz_ctx* ctx, rz_keyindex* ix, void* d_data, int64_t n, uint32_t record_bytes,
+                     const uint64_t* d_keys, int64_t k, int64_t* new_len, uint32_t flags, rz_stream_t stream);
+
+/*
  * O(n) stable partition comparator (mark, per-tile counts and their scan, then a pipelined
  * in-place move), in place. Survivors keep their relative order, as with thrust::remove
  * (Thrust_remove.hxx:15-17) and InK compact (cuCompactor.cuh:104-141).

@@ -235,6 +235,58 @@ def remove_batched(ctx: Context, lists, stream=None) -> None:
                                              ctypes.c_void_p(_stream_handle(stream))), "rz_remove_batched")
 
 
+class KeyIndex:
+    """Key -> row index of a table whose records begin with a uint64 key (rz_keyindex_*), kept
+    exact by `remove_by_key`."""
+
+    def __init__(self, ctx: Context, capacity: int):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx._check(_native.lib.rz_keyindex_create(ctx.handle, int(capacity), ctypes.byref(h)), "rz_keyindex_create")
+        self.handle = h
+
+    def build(self, table, n: int | None = None, stream=None) -> None:
+        n = int(table.shape[0]) if n is None else int(n)
+        self.ctx._check(_native.lib.rz_keyindex_build(self.handle, ctypes.c_void_p(table.data_ptr()), n,
+                                                      item_bytes(table), ctypes.c_void_p(_stream_handle(stream))),
+                        "rz_keyindex_build")
+
+    def insert(self, table, first: int, count: int, stream=None) -> None:
+        self.ctx._check(_native.lib.rz_keyindex_insert(self.handle, ctypes.c_void_p(table.data_ptr()), int(first),
+                                                       int(count), item_bytes(table),
+                                                       ctypes.c_void_p(_stream_handle(stream))), "rz_keyindex_insert")
+
+    def find(self, keys, stream=None):
+        """Rows (int64 tensor, -1 when absent) of a CUDA int64 tensor of keys."""
+        import torch
+        rows = torch.empty(keys.numel(), dtype=torch.int32, device=keys.device)
+        self.ctx._check(_native.lib.rz_keyindex_find(self.handle, ctypes.c_void_p(keys.data_ptr()), keys.numel(),
+                                                     ctypes.c_void_p(rows.data_ptr()),
+                                                     ctypes.c_void_p(_stream_handle(stream))), "rz_keyindex_find")
+        r = rows.to(torch.int64) & 0xFFFFFFFF
+        r[r == 0xFFFFFFFF] = -1
+        return r
+
+    def remove_by_key(self, table, n: int, keys, flags: int = 0, stream=None) -> int:
+        out = ctypes.c_int64(0)
+        self.ctx._check(_native.lib.rz_remove_by_key(self.ctx.handle, self.handle, ctypes.c_void_p(table.data_ptr()),
+                                                     int(n), item_bytes(table), ctypes.c_void_p(keys.data_ptr()),
+                                                     keys.numel(), ctypes.byref(out), flags,
+                                                     ctypes.c_void_p(_stream_handle(stream))), "rz_remove_by_key")
+        return out.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _native.lib.rz_keyindex_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Service:
     """Streaming delete service over a device-resident table (rz_service_*).
 

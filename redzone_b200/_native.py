@@ -86,6 +86,12 @@ _sig("rz_remove_host_idx", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes
 _sig("rz_append_remove", c_i32, [c_vp, c_vp, c_i64, c_i64, c_u32, c_vp, c_i64, c_vp, c_i64, ctypes.POINTER(c_i64),
                                   c_u32, c_vp])
 _sig("rz_keep", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
+_sig("rz_keyindex_create", c_i32, [c_vp, c_i64, ctypes.POINTER(c_vp)])
+_sig("rz_keyindex_destroy", None, [c_vp])
+_sig("rz_keyindex_build", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp])
+_sig("rz_keyindex_insert", c_i32, [c_vp, c_vp, c_i64, c_i64, c_u32, c_vp])
+_sig("rz_keyindex_find", c_i32, [c_vp, c_vp, c_i64, c_vp, c_vp])
+_sig("rz_remove_by_key", c_i32, [c_vp, c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
 _sig("rz_partition", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
 _sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchCfg)])
 _sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
