@@ -621,6 +621,17 @@ def main():
     ap.add_argument("--lists", type=int, default=4096, help="--workload batched: number of lists")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true", help="--workload batched: skip the autotuner")
+    ap.add_argument("--config", default=None,
+                    help="JSON file of option defaults, e.g. {\"workload\": \"service\", \"rate\": 40000}; "
+                         "flags on the command line override it")
+    pre, _ = ap.parse_known_args()
+    if pre.config:
+        cfg = json.loads(Path(pre.config).read_text())
+        known = {a.dest for a in ap._actions}
+        unknown = sorted(set(cfg) - known)
+        if unknown:
+            ap.error(f"unknown keys in {pre.config}: {unknown}")
+        ap.set_defaults(**cfg)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

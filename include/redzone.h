@@ -86,6 +86,11 @@ int  rz_last_cuda_error(const rz_ctx* ctx, char* buf, size_t len);
 int  rz_sync_status(rz_ctx* ctx, rz_stream_t stream);
 /* Number of SMs of the context's device. */
 int  rz_num_sms(const rz_ctx* ctx);
+/* Cap the context scratch the library may grow (bytes; negative = no cap). A call that would need
+ * more returns RZ_ERR_NO_MEMORY and changes nothing; scratch already held is kept. Also the way
+ * tests inject an allocation failure. rz_scratch_bytes reports what the context holds. */
+int  rz_set_scratch_limit(rz_ctx* ctx, int64_t bytes);
+int64_t rz_scratch_bytes(const rz_ctx* ctx);
 
 /* ---- single list -------------------------------------------------------------------------- */
 /*
@@ -265,6 +270,13 @@ int  rz_service_stats_get(rz_service* svc, rz_service_stats* out);
 int  rz_service_reset_stats(rz_service* svc);
 /* Live lengths as the host plans them and as the device tracks them (either pointer may be NULL). */
 int  rz_service_lengths(rz_service* svc, int64_t* host_view, int64_t* device_view);
+/* Checkpoint / resume. rz_service_checkpoint drains (up to timeout_ms), then writes every shard's
+ * live length and the count of records refills have appended to it (both `shards` entries); with
+ * the caller's copy of its table (rows [0, length) of each shard) that is the whole state.
+ * rz_service_restore loads such a state into an idle service (RZ_ERR_BUSY if work is pending);
+ * later refills then append exactly the records the original service would have. */
+int  rz_service_checkpoint(rz_service* svc, int64_t* lengths, int64_t* appended, int32_t timeout_ms);
+int  rz_service_restore(rz_service* svc, const int64_t* lengths, const int64_t* appended);
 void rz_service_destroy(rz_service* svc);
 /* Load generator: Poisson arrivals at `rate` batches/s for `seconds`; each arrival submits a random
  * batch of `pool` (pinned index arrays, lent to the service) to a uniformly random shard; then

@@ -80,6 +80,15 @@ class Context:
     def num_sms(self) -> int:
         return _native.lib.rz_num_sms(self.handle)
 
+    def set_scratch_limit(self, nbytes: int | None) -> None:
+        """Cap the scratch this context may grow (None: no cap)."""
+        self._check(_native.lib.rz_set_scratch_limit(self.handle, -1 if nbytes is None else int(nbytes)),
+                    "rz_set_scratch_limit")
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(_native.lib.rz_scratch_bytes(self.handle))
+
     def remove(self, data, idx, flags: int = 0, stream=None) -> int:
         """In-place Redzone removal; returns the new length (n - k)."""
         n, k = int(data.shape[0]), int(idx.numel())
@@ -344,6 +353,18 @@ class Service:
         d = (ctypes.c_int64 * self.shards)()
         self.ctx._check(_native.lib.rz_service_lengths(self.handle, h, d), "rz_service_lengths")
         return list(h), list(d)
+
+    def checkpoint(self, timeout_ms: int = 600000) -> tuple[list[int], list[int]]:
+        """Drain, then (live lengths, refill-appended counts) per shard."""
+        ln = (ctypes.c_int64 * self.shards)()
+        ap = (ctypes.c_int64 * self.shards)()
+        self.ctx._check(_native.lib.rz_service_checkpoint(self.handle, ln, ap, timeout_ms), "rz_service_checkpoint")
+        return list(ln), list(ap)
+
+    def restore(self, lengths, appended) -> None:
+        ln = (ctypes.c_int64 * self.shards)(*[int(x) for x in lengths])
+        ap = (ctypes.c_int64 * self.shards)(*[int(x) for x in appended])
+        self.ctx._check(_native.lib.rz_service_restore(self.handle, ln, ap), "rz_service_restore")
 
     def run_poisson(self, pool, rate: float, seconds: float, seed: int = 0) -> dict:
         """Poisson arrivals of random pool batches (pinned CPU tensors) to random shards."""

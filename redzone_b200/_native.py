@@ -80,6 +80,8 @@ _sig("rz_status_string", c_i32, [c_i32, ctypes.c_char_p, ctypes.c_size_t])
 _sig("rz_last_cuda_error", c_i32, [c_vp, ctypes.c_char_p, ctypes.c_size_t])
 _sig("rz_sync_status", c_i32, [c_vp, c_vp])
 _sig("rz_num_sms", c_i32, [c_vp])
+_sig("rz_set_scratch_limit", c_i32, [c_vp, c_i64])
+_sig("rz_scratch_bytes", c_i64, [c_vp])
 _sig("rz_remove", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
 _sig("rz_remove_cfg", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(LaunchCfg), c_u32, c_vp])
 _sig("rz_remove_host_idx", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_u32, c_vp])
@@ -137,6 +139,8 @@ _sig("rz_service_stats_get", c_i32, [c_vp, ctypes.POINTER(ServiceStats)])
 _sig("rz_service_reset_stats", c_i32, [c_vp])
 _sig("rz_service_lengths", c_i32, [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)])
 _sig("rz_service_destroy", None, [c_vp])
+_sig("rz_service_checkpoint", c_i32, [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64), c_i32])
+_sig("rz_service_restore", c_i32, [c_vp, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64)])
 _sig("rz_service_run_poisson", c_i32, [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_i64), c_i32, ctypes.c_double,
                                        ctypes.c_double, c_u64, ctypes.POINTER(ServiceStats)])
 

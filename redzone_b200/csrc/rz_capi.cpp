@@ -24,9 +24,20 @@ static int grow(rz_ctx* ctx, T*& ptr, size_t& cap, size_t want, bool zero) {
     if (want <= cap && ptr) return RZ_OK;
     size_t nc = std::max<size_t>(want, cap * 2);
     nc = std::max<size_t>(nc, 1024);
+    // The scratch limit (rz_set_scratch_limit) counts every grown buffer; refusing leaves the old
+    // buffer in place, so a refused call changes nothing.
+    const size_t held_after = ctx->scratch_held - (ptr ? cap * sizeof(T) : 0) + nc * sizeof(T);
+    if (held_after > ctx->scratch_limit) {
+        if (want * sizeof(T) + ctx->scratch_held - (ptr ? cap * sizeof(T) : 0) > ctx->scratch_limit) {
+            ctx->last_cuda_error = "context scratch limit reached";
+            return RZ_ERR_NO_MEMORY;
+        }
+        nc = want;  // the doubling would pass the limit; the exact size still fits
+    }
     if (ptr) {
         RZ_CUDA_TRY(ctx, cudaDeviceSynchronize());
         RZ_CUDA_TRY(ctx, cudaFree(ptr));
+        ctx->scratch_held -= cap * sizeof(T);
         ptr = nullptr;
         cap = 0;
     }
@@ -35,6 +46,7 @@ static int grow(rz_ctx* ctx, T*& ptr, size_t& cap, size_t want, bool zero) {
     if (zero) RZ_CUDA_TRY(ctx, cudaMemset(p, 0, nc * sizeof(T)));
     ptr = static_cast<T*>(p);
     cap = nc;
+    ctx->scratch_held += nc * sizeof(T);
     return RZ_OK;
 }
 
@@ -239,6 +251,15 @@ int rz_sync_status(rz_ctx* ctx, rz_stream_t stream) {
 }
 
 int rz_num_sms(const rz_ctx* ctx) { return ctx ? ctx->sms : 0; }
+
+int rz_set_scratch_limit(rz_ctx* ctx, int64_t bytes) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    ctx->scratch_limit = bytes < 0 ? ~size_t(0) : size_t(bytes);
+    return RZ_OK;
+}
+
+int64_t rz_scratch_bytes(const rz_ctx* ctx) { return ctx ? int64_t(ctx->scratch_held) : 0; }
 
 int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes, rz_launch_cfg* cfg) {
     if (!ctx || !cfg || k < 0 || n < k) return RZ_ERR_INVALID_ARG;

@@ -68,6 +68,8 @@ struct rz_ctx {
     int last_block = 0;
     void* predictor = nullptr;   // rz::Predictor*, owned (see rz_mlp.cu)
     void* tune_table = nullptr;  // rz::TuneTable*, owned (see rz_autotune.cpp)
+    size_t scratch_held = 0;     // bytes of grown context scratch
+    size_t scratch_limit = ~size_t(0);  // rz_set_scratch_limit: growth beyond it -> RZ_ERR_NO_MEMORY
 };
 
 namespace rz {

@@ -373,6 +373,31 @@ int rz_service_lengths(rz_service* S, int64_t* host_view, int64_t* device_view) 
     return RZ_OK;
 }
 
+int rz_service_checkpoint(rz_service* S, int64_t* lengths, int64_t* appended, int32_t timeout_ms) {
+    if (!S || !lengths || !appended) return RZ_ERR_INVALID_ARG;
+    const int st = rz_service_drain(S, timeout_ms);
+    if (st != RZ_OK) return st;
+    std::lock_guard<std::mutex> g(S->mu);
+    std::memcpy(lengths, S->len.data(), 8 * S->len.size());
+    std::memcpy(appended, S->appended.data(), 8 * S->appended.size());
+    return RZ_OK;
+}
+
+int rz_service_restore(rz_service* S, const int64_t* lengths, const int64_t* appended) {
+    if (!S || !lengths || !appended) return RZ_ERR_INVALID_ARG;
+    for (size_t s = 0; s < S->len.size(); ++s)
+        if (lengths[s] < 0 || lengths[s] > S->cfg.shard_capacity || appended[s] < 0) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> g(S->mu);
+    if (S->in_flight != 0) return RZ_ERR_BUSY;
+    for (const Slot& slot : S->slots)
+        if (slot.busy) return RZ_ERR_BUSY;
+    std::memcpy(S->len.data(), lengths, 8 * S->len.size());
+    std::memcpy(S->appended.data(), appended, 8 * S->appended.size());
+    cudaSetDevice(S->ctx->device);
+    RZ_CUDA_TRY(S->ctx, cudaMemcpy(S->d_len, S->len.data(), 8 * S->len.size(), cudaMemcpyHostToDevice));
+    return RZ_OK;
+}
+
 void rz_service_destroy(rz_service* S) {
     if (!S) return;
     {

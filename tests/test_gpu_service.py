@@ -100,6 +100,39 @@ def test_each_result_is_the_same_alone_and_in_the_mix(ctx):
         assert np.array_equal(mix[s, : mlen[s]], exp[s, : elen[s]]), s
 
 
+def test_checkpoint_and_resume_give_the_same_tables(ctx):
+    """Checkpoint half-way (lengths, refill counters, the caller's copy of its table), resume in a
+    new service, apply the second half: the tables equal those of one uninterrupted run."""
+    seq = batches(21, 1200)  # ~268 rows per batch: each shard refills after ~61 of its batches
+    first, second = seq[:700], seq[700:]
+    full, flen, _, _ = run_service(ctx, seq, slots=4, max_batches=8, one_at_a_time=False)
+
+    table = torch.from_numpy(initial_table().view(np.int32)).to(DEV)
+    svc = rz.Service(ctx, table, SHARDS, CAP, slots=4, max_batches_per_launch=8, index_budget_bytes=8 << 20,
+                     floor_rows=FLOOR)
+    for shard, idx in first:
+        svc.submit(shard, idx)
+    lengths, appended = svc.checkpoint()
+    saved = table.cpu().clone()  # the caller's own copy of its table
+    svc.close()
+    assert any(a > 0 for a in appended)  # refills happened before the checkpoint
+
+    table2 = saved.to(DEV)
+    svc2 = rz.Service(ctx, table2, SHARDS, CAP, slots=2, max_batches_per_launch=4, index_budget_bytes=8 << 20,
+                      floor_rows=FLOOR)
+    svc2.restore(lengths, appended)
+    for shard, idx in second:
+        svc2.submit(shard, idx)
+    svc2.drain()
+    h, d = svc2.lengths()
+    svc2.close()
+    torch.cuda.synchronize()
+    assert h == d == flen
+    got = table2.cpu().numpy().view(np.uint32).reshape(SHARDS, CAP, WORDS)
+    for s in range(SHARDS):
+        assert np.array_equal(got[s, : h[s]], full[s, : flen[s]]), s
+
+
 def test_statistics_and_admission_limit(ctx):
     table = torch.zeros((SHARDS * CAP, WORDS), dtype=torch.int32, device=DEV)
     svc = rz.Service(ctx, table, SHARDS, CAP, slots=2, max_batches_per_launch=4, index_budget_bytes=2 * 4 * 1000,

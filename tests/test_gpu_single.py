@@ -115,6 +115,43 @@ def test_edge_sizes(ctx, n, k):
     assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
 
 
+def test_exhaustive_tiny_lists_every_schedule(ctx):
+    """Every ordered removal list of every length for n <= 5, through the single-CTA, cluster and
+    grid schedules (the grid with 32-item tiles, so n = 5 already spans CTAs only at k > 32 -- see
+    the n = 64 case below), against the oracle."""
+    import itertools
+    schedules = [("block", None, rz.RZ_FORCE_BLOCK), ("auto", None, 0),
+                 ("grid32", rz.LaunchCfg(32, 1, 4, 0, 3), rz.RZ_FORCE_GRID)]
+    count = 0
+    for n in range(1, 6):
+        host = np.arange(100 * n, 100 * n + n, dtype=np.uint32).reshape(n, 1)
+        for k in range(n + 1):
+            for perm in itertools.permutations(range(n), k):
+                idx = np.array(perm, dtype=np.uint32)
+                exp = expect_of(host, idx)
+                for name, cfg, flags in schedules:
+                    got = run_gpu(ctx, host, idx, cfg=cfg, flags=flags | rz.RZ_SYNC)
+                    assert np.array_equal(got[: n - k], exp[: n - k]), (name, n, perm)
+                count += 1
+    assert count == sum(len(list(itertools.permutations(range(n), k))) for n in range(1, 6) for k in range(n + 1))
+
+
+@pytest.mark.parametrize("words", [1, 4])
+def test_n64_every_k_multi_cta(ctx, words):
+    """n = 64 with 32-item tiles: every k, several orders each, so grids of 1-2 CTAs run both the
+    red-list and the bitmap paths (k = 64 .. 33 have up to 31 red entries per CTA)."""
+    n = 64
+    rng = np.random.default_rng(words)
+    host = payload(n, words, seed=5)
+    for k in range(n + 1):
+        for rep in range(4):
+            idx = rng.permutation(n)[:k].astype(np.uint32)
+            exp = expect_of(host, idx)
+            for cfg in (rz.LaunchCfg(32, 1, 4, 0, 3), rz.LaunchCfg(32, 2, 4, 0, 3)):
+                got = run_gpu(ctx, host, idx, cfg=cfg, flags=rz.RZ_FORCE_GRID | rz.RZ_SYNC)
+                assert np.array_equal(got[: n - k], exp[: n - k]), (words, k, rep, cfg)
+
+
 def test_back_to_back_calls_leave_scratch_clean(ctx):
     """Bitmap and barrier state are self-cleaning: many calls in a row stay exact."""
     rng = np.random.default_rng(0)
@@ -273,6 +310,31 @@ def test_append_then_remove(ctx):
         got = d.cpu().numpy().view(np.uint32)
         assert np.array_equal(got[:new_len], grown[:new_len]), (words, n, g, k)
         assert np.array_equal(got[n + g:], host[n + g:])  # past the grown list: untouched
+
+
+def test_allocation_failure_is_a_status_and_changes_nothing():
+    """Injected allocation failure: with a scratch cap of 0 bytes a fresh context cannot grow its
+    scratch, so the call returns RZ_ERR_NO_MEMORY with the data untouched; lifting the cap makes
+    the same context work."""
+    c = rz.Context(0)
+    n, k = 1 << 16, 1 << 12
+    host = payload(n, 1, seed=3)
+    idx = workloads.uniform(n, k, seed=4)
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    di = torch.from_numpy(idx.astype(np.int32)).to(DEV)
+    c.set_scratch_limit(0)
+    for call in (lambda: c.remove(d, di, flags=rz.RZ_SYNC), lambda: c.partition(d, di, flags=rz.RZ_SYNC),
+                 lambda: c.keep(d, di, flags=rz.RZ_SYNC)):
+        with pytest.raises(rz.RedzoneError) as e:
+            call()
+        assert e.value.code == 4  # RZ_ERR_NO_MEMORY
+    assert c.scratch_bytes == 0
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), host)
+    c.set_scratch_limit(None)
+    assert c.remove(d, di, flags=rz.RZ_SYNC) == n - k
+    assert np.array_equal(d.cpu().numpy().view(np.uint32)[: n - k], expect_of(host, idx)[: n - k])
+    assert c.scratch_bytes > 0
+    c.close()
 
 
 def test_bounded_barrier_wait_times_out_with_status(ctx):
