@@ -36,7 +36,10 @@ def run_gpu(ctx, host, idx, cfg=None, flags=rz.RZ_SYNC):
         ctx.remove_cfg(d, di, cfg, flags=flags)
     torch.cuda.synchronize()
     assert torch.equal(di, di_before), "the removal list must not be written"
-    return d.cpu().numpy().view(np.uint32)
+    got = d.cpu().numpy().view(np.uint32)
+    k = int(idx.size)
+    assert np.array_equal(got[host.shape[0] - k:], host[host.shape[0] - k:]), "the tail must not be written"
+    return got
 
 
 def expect_of(host, idx):
