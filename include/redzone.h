@@ -63,6 +63,7 @@ typedef enum rz_status {
 #define RZ_SCHED_BLOCK   1  /* one CTA, block-level synchronisation                              */
 #define RZ_SCHED_CLUSTER 2  /* one thread-block cluster; red-zone bitmap in distributed smem      */
 #define RZ_SCHED_GRID    3  /* persistent grid, bounded global barriers                           */
+#define RZ_SCHED_CSCAN   4  /* independent 8-CTA clusters, each finds every red entry; no grid wait */
 
 /* Launch configuration of the single-list kernels (one entry of the 48-point tuning space:
  * block x items x grid scale, plus the Redzone-vs-partition bit). */

@@ -102,6 +102,8 @@ int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint
                      uint32_t k, uint32_t flags, cudaStream_t s, LaunchInfo* info);
 // Cluster schedule (rz_cluster.cu); RZ_ERR_UNSUPPORTED when the bitmap slice does not fit in
 // shared memory or no cluster of the requested size can be co-scheduled.
+int launch_cscan(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
+                 const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                    const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int cluster_max_block(int w, int items);

@@ -71,10 +71,10 @@ def test_widths_and_distributions(ctx, words, dist):
         assert np.array_equal(got[n - k:], host[n - k:]), "tail must be left untouched"
 
 
-SCHEDULES = {"cluster": 2, "grid": 3}
+SCHEDULES = {"cluster": 2, "grid": 3, "cscan": 4}
 
 
-@pytest.mark.parametrize("sched", ["cluster", "grid"])
+@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan"])
 def test_every_launch_config_gives_the_same_bits(ctx, sched):
     """The result depends only on (data, idx), never on schedule, block, items or grid."""
     cases = [(1 << 20, 1 << 16, "uniform"), (1 << 18, 1 << 17, "red50"), (1 << 16, 3001, "red100")]
@@ -91,7 +91,7 @@ def test_every_launch_config_gives_the_same_bits(ctx, sched):
                         assert np.array_equal(got[: n - k], exp[: n - k]), (sched, n, k, dist, words, block, items, cps)
 
 
-@pytest.mark.parametrize("sched", ["cluster", "grid"])
+@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan"])
 @pytest.mark.parametrize("words", [1, 2, 4, 8])
 def test_schedules_on_large_k(ctx, sched, words):
     n = 1 << 21
@@ -150,8 +150,9 @@ def test_n64_every_k_multi_cta(ctx, words):
         for rep in range(4):
             idx = rng.permutation(n)[:k].astype(np.uint32)
             exp = expect_of(host, idx)
-            for cfg in (rz.LaunchCfg(32, 1, 4, 0, 3), rz.LaunchCfg(32, 2, 4, 0, 3)):
-                got = run_gpu(ctx, host, idx, cfg=cfg, flags=rz.RZ_FORCE_GRID | rz.RZ_SYNC)
+            for cfg, fl in ((rz.LaunchCfg(32, 1, 4, 0, 3), rz.RZ_FORCE_GRID), (rz.LaunchCfg(32, 2, 4, 0, 3), rz.RZ_FORCE_GRID),
+                            (rz.LaunchCfg(32, 1, 4, 0, 4), 0), (rz.LaunchCfg(32, 4, 1, 0, 4), 0)):
+                got = run_gpu(ctx, host, idx, cfg=cfg, flags=fl | rz.RZ_SYNC)
                 assert np.array_equal(got[: n - k], exp[: n - k]), (words, k, rep, cfg)
 
 
@@ -186,6 +187,25 @@ def test_validation_reports_and_leaves_data_untouched(ctx):
     assert np.array_equal(d.cpu().numpy().view(np.uint32), host)
     # A valid call right after the failures still gives the exact result.
     got = run_gpu(ctx, host, idx, flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
+def test_validation_on_the_cluster_scan_schedule(ctx):
+    """A failed validation on the cluster-scan schedule leaves the data untouched (its CTAs still
+    meet at both cluster barriers), and the next call is exact."""
+    n, k = 1 << 18, 1 << 14
+    host = payload(n, 2, seed=9)
+    idx = workloads.uniform(n, k, seed=9)
+    cfg = rz.LaunchCfg(256, 4, 1, 0, 4)
+    for bad_at, bad_val, code in ((100, None, 2), (7, n + 3, 3)):
+        bad = idx.copy()
+        bad[bad_at] = bad[bad_at + 1] if bad_val is None else bad_val
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        with pytest.raises(rz.RedzoneError) as e:
+            ctx.remove_cfg(d, torch.from_numpy(bad.astype(np.int32)).to(DEV), cfg, flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+        assert e.value.code == code
+        assert np.array_equal(d.cpu().numpy().view(np.uint32).reshape(n, 2), host)
+    got = run_gpu(ctx, host, idx, cfg=cfg, flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
     assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
 
 
@@ -244,7 +264,8 @@ def test_red_list_schedule_around_its_limit(ctx, red, words):
     rng.shuffle(idx)
     host = payload(n, words, seed=red)
     exp = expect_of(host, idx)
-    for cfg in (None, rz.LaunchCfg(256, 4, 1, 0, 3), rz.LaunchCfg(128, 2, 4, 0, 3)):
+    for cfg in (None, rz.LaunchCfg(256, 4, 1, 0, 3), rz.LaunchCfg(128, 2, 4, 0, 3), rz.LaunchCfg(256, 4, 1, 0, 4),
+                rz.LaunchCfg(128, 2, 4, 0, 4), rz.LaunchCfg(64, 1, 4, 0, 4)):
         got = run_gpu(ctx, host, idx, cfg=cfg)
         assert np.array_equal(got[: n - k], exp[: n - k]), (red, words, cfg)
 
