@@ -100,10 +100,17 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
                    LaunchInfo* info);
 int launch_partition(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx,
                      uint32_t k, uint32_t flags, cudaStream_t s, LaunchInfo* info);
-// Cluster schedule (rz_cluster.cu); RZ_ERR_UNSUPPORTED when the bitmap slice does not fit in
-// shared memory or no cluster of the requested size can be co-scheduled.
+// Cluster-scan schedule (rz_cscan.cu); RZ_ERR_UNSUPPORTED when a slice of the index list does not
+// fit one register pass, the maps do not fit in shared memory, the index list is not 16-byte
+// aligned or no cluster can be co-scheduled.
 int launch_cscan(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                  const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
+// The default cluster-scan launch for (k, w), if that schedule runs it: false otherwise.
+bool cscan_default_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
+constexpr uint32_t kCscanMinK = (1u << 12) + 1;  // the default uses the cluster scan from here
+constexpr uint32_t kCscanMaxK = 1u << 17;       // ... to here (one register pass per slice)
+// Cluster schedule (rz_cluster.cu); RZ_ERR_UNSUPPORTED when the bitmap slice does not fit in
+// shared memory or no cluster of the requested size can be co-scheduled.
 int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                    const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int cluster_max_block(int w, int items);

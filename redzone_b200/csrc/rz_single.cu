@@ -155,10 +155,13 @@ int default_cfg(const rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch
     (void)n;
     cfg->use_partition = 0;
     cfg->schedule = RZ_SCHED_AUTO;
-    // Measured on B200 (n = 2^28, int32 and 16-byte items, L2 flushed, exhaustive autotune): the
-    // 16-CTA cluster wins up to k = 2^14; above that the grid schedule with 512-item tiles at 2^15,
-    // 1024-item tiles to 2^17 (64 CTAs at 2^16 -- fewer, fuller CTAs shorten the grid-wide wait),
-    // and 4096-item tiles on two CTAs per SM beyond.
+    // Measured on B200 (n = 2^28, L2 flushed): the cluster-scan schedule, which needs no grid-wide
+    // wait, wins from k = 2^13 to 2^17 (7.2 against 11.1 us per call at k = 2^16, graph steady
+    // state); below that the 16-CTA cluster schedule. Where the cluster scan does not run (wider
+    // items at k > 2^16, k > 2^17): the grid schedule with 512-item tiles at 2^15, 1024-item tiles
+    // to 2^17 (64 CTAs at 2^16 -- fewer, fuller CTAs shorten the grid-wide wait), and 4096-item
+    // tiles on two CTAs per SM beyond.
+    if (k >= kCscanMinK && cscan_default_cfg(ctx, k, w, cfg)) return RZ_OK;
     if (k <= kClusterMaxK) {
         cfg->block = 256; cfg->items = 4; cfg->ctas_per_sm = 4;
     } else if (k <= (1u << 15)) {

@@ -192,7 +192,7 @@ def test_validation_reports_and_leaves_data_untouched(ctx):
 
 def test_validation_on_the_cluster_scan_schedule(ctx):
     """A failed validation on the cluster-scan schedule leaves the data untouched (its CTAs still
-    meet at both cluster barriers), and the next call is exact."""
+    meet at every cluster barrier phase), and the next call is exact."""
     n, k = 1 << 18, 1 << 14
     host = payload(n, 2, seed=9)
     idx = workloads.uniform(n, k, seed=9)
@@ -268,6 +268,36 @@ def test_red_list_schedule_around_its_limit(ctx, red, words):
                 rz.LaunchCfg(128, 2, 4, 0, 4), rz.LaunchCfg(64, 1, 4, 0, 4)):
         got = run_gpu(ctx, host, idx, cfg=cfg)
         assert np.array_equal(got[: n - k], exp[: n - k]), (red, words, cfg)
+
+
+@pytest.mark.parametrize("red", [255, 256, 257, 1024])
+def test_cluster_scan_push_region_limit(ctx, red):
+    """All `red` red entries in the first slice of the index list: up to 256 per slice the
+    cluster-scan schedule pushes them to every cluster member, above that it ORs the partial maps;
+    the results are the canonical ones either way."""
+    n, k = 1 << 20, 1 << 15
+    cut = n - k
+    rng = np.random.default_rng(red)
+    idx = np.concatenate([cut + rng.choice(k, size=red, replace=False),
+                          rng.choice(cut, size=k - red, replace=False)]).astype(np.uint32)
+    host = payload(n, 2, seed=red)
+    exp = expect_of(host, idx)
+    for cfg in (rz.LaunchCfg(256, 4, 1, 0, 4), rz.LaunchCfg(512, 1, 1, 0, 4)):
+        got = run_gpu(ctx, host, idx, cfg=cfg)
+        assert np.array_equal(got[: n - k], exp[: n - k]), (red, cfg)
+
+
+def test_cluster_scan_with_an_unaligned_index_list(ctx):
+    """An index list that does not start on a 16-byte boundary runs on the grid schedule instead
+    (the cluster scan reads it in 16-byte units), with the same result."""
+    n, k = 1 << 20, 1 << 14
+    host = payload(n, 1, seed=4)
+    idx = workloads.uniform(n, k, seed=4)
+    buf = torch.from_numpy(np.concatenate([[0], idx]).astype(np.int32)).to(DEV)
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    ctx.remove_cfg(d, buf[1:], rz.LaunchCfg(256, 4, 1, 0, 4), flags=rz.RZ_SYNC)
+    got = d.cpu().numpy().view(np.uint32).reshape(n, 1)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
 
 
 def test_partition_more_tiles_than_one_scan_chunk(ctx):
