@@ -16,12 +16,12 @@ from __future__ import annotations
 import ctypes
 
 from . import _native
-from ._native import (LaunchCfg, RZ_ALLOW_STABLE, RZ_FORCE_BLOCK, RZ_FORCE_GRID, RZ_FORCE_PARTITION,
-                      RZ_SYNC, RZ_USE_PREDICTOR, RZ_VALIDATE, status_string)
+from ._native import (LaunchCfg, RZ_ALLOW_STABLE, RZ_CLOBBER_INDICES, RZ_FORCE_BLOCK, RZ_FORCE_GRID,
+                      RZ_FORCE_PARTITION, RZ_SYNC, RZ_USE_PREDICTOR, RZ_VALIDATE, status_string)
 
 __all__ = ["Context", "RedzoneError", "LaunchCfg", "RemoveFromList", "remove", "default_context",
            "RZ_VALIDATE", "RZ_SYNC", "RZ_FORCE_PARTITION", "RZ_FORCE_BLOCK", "RZ_FORCE_GRID",
-           "RZ_USE_PREDICTOR", "RZ_ALLOW_STABLE", "item_bytes"]
+           "RZ_USE_PREDICTOR", "RZ_ALLOW_STABLE", "RZ_CLOBBER_INDICES", "item_bytes"]
 
 
 class RedzoneError(RuntimeError):

@@ -50,6 +50,7 @@ RZ_FORCE_BLOCK = 0x8
 RZ_FORCE_GRID = 0x10
 RZ_USE_PREDICTOR = 0x20
 RZ_ALLOW_STABLE = 0x40
+RZ_CLOBBER_INDICES = 0x80  # accepted; the index list is never written
 
 
 class ListDesc(ctypes.Structure):

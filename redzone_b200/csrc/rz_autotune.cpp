@@ -2,9 +2,9 @@
 //
 // The reference fixes its launch configuration at compile time (GPUBlockCount / GPUBlockSize,
 // tests.cu:1-2; prefetch depth 5, redzone.hxx:1134). Here every call can pick its configuration:
-// rz_autotune_single times the 48-point space (block 128/256/512/1024 x items per thread 1/2/4/8
-// x grid scale 1/2/4) plus the O(n) partition path with CUDA events and an L2 flush between
-// repetitions; rz_autotune_batched does the same for the batched kernel's tile and grid. The
+// rz_autotune_single times the 56-point space (block 128/256/512/1024 x items per thread 1/2/4/8
+// x grid scale 1/2/4 with the schedule chosen by k, and eight cluster-scan launches) plus the
+// O(n) partition path with CUDA events and an L2 flush between repetitions; rz_autotune_batched does the same for the batched kernel's tile and grid. The
 // winners go into a per-context table keyed by (payload width, log2 k) that rz_remove and
 // rz_batch_plan_create consult, and which can be saved to and loaded from a text file.
 #include <algorithm>
@@ -90,15 +90,19 @@ static int ensure_scrub(rz_ctx* ctx) {
     return RZ_OK;
 }
 
-// The 48-point space in a fixed order (the predictor's class index is the position here).
-void config_space(rz_launch_cfg* out48) {
+// The space in a fixed order (the predictor's class index is the position here). A cluster-scan
+// point that does not run for an instance (k > 2^17, a slice too long for the block, wide items
+// on 512 threads, a misaligned index list) runs the grid schedule with the same block and items.
+void config_space(rz_launch_cfg* out) {
     static const int blocks[4] = {128, 256, 512, 1024};
     static const int items[4] = {1, 2, 4, 8};
     static const int gs[3] = {1, 2, 4};
+    static const int cscan[8][2] = {{128, 2}, {128, 4}, {256, 1}, {256, 2}, {256, 4}, {256, 8}, {512, 2}, {512, 4}};
     int q = 0;
     for (int b : blocks)
         for (int i : items)
-            for (int g : gs) out48[q++] = rz_launch_cfg{b, i, g, 0, RZ_SCHED_AUTO};
+            for (int g : gs) out[q++] = rz_launch_cfg{b, i, g, 0, RZ_SCHED_AUTO};
+    for (const auto& c : cscan) out[q++] = rz_launch_cfg{c[0], c[1], 2, 0, RZ_SCHED_CSCAN};
 }
 
 }  // namespace rz
@@ -115,16 +119,16 @@ int rz_autotune_single(rz_ctx* ctx, void* d_data, int64_t n, uint32_t w, const u
     int st = ensure_scrub(ctx);
     if (st != RZ_OK) return st;
     TuneTable* t = table(ctx);
-    rz_launch_cfg space[49];
+    rz_launch_cfg space[kConfigSpace + 1];
     config_space(space);
-    space[48] = rz_launch_cfg{256, 8, 1, 1, RZ_SCHED_AUTO};
+    space[kConfigSpace] = rz_launch_cfg{256, 8, 1, 1, RZ_SCHED_AUTO};  // the partition path
     cudaStream_t s = nullptr;
     RZ_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     std::vector<rz_tune_entry> res;
-    for (int q = 0; q < 49; ++q) {
+    for (int q = 0; q <= kConfigSpace; ++q) {
         std::vector<float> ms;
         st = rz_remove_cfg(ctx, d_data, n, w, d_idx, k, &space[q], 0, reinterpret_cast<rz_stream_t>(s));  // warm-up
         if (st != RZ_OK) break;

@@ -115,8 +115,10 @@ int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
                    const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int cluster_max_block(int w, int items);
 constexpr uint32_t kClusterMaxK = 1u << 14;  // RZ_SCHED_AUTO uses the cluster schedule up to here
-// The 48-point launch-configuration space in its canonical order (rz_autotune.cpp).
-void config_space(rz_launch_cfg* out48);
+// The launch-configuration space in its canonical order (rz_autotune.cpp): 48 grid / cluster
+// points (block x items x grid scale, schedule chosen by k) and 8 cluster-scan points.
+constexpr int kConfigSpace = 56;
+void config_space(rz_launch_cfg* out);
 int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cudaStream_t s);
 // rz_keep: gather data[keep[j]] into `stage` (m items), then copy the stage to data[0..m).
 int launch_keep(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* keep, uint32_t m, void* stage,

@@ -1,8 +1,8 @@
 // rz_mlp.cu -- learned launch-configuration predictor: features, FP32 MLP training and inference.
 //
-// The network maps 12 features of a removal instance to 48 logits (softmax over the launch
+// The network maps 12 features of a removal instance to 56 logits (softmax over the launch
 // configurations of config_space(), rz_autotune.cpp) plus one logit for "the O(n) partition
-// path beats Redzone". Layers: 12 -> 64 (ReLU) -> 64 (ReLU) -> 49. All arithmetic is FP32 in
+// path beats Redzone". Layers: 12 -> 64 (ReLU) -> 64 (ReLU) -> 57. All arithmetic is FP32 in
 // hand-written kernels (no cuBLAS): one warp per sample for the forward and backward passes
 // with the weights staged in shared memory, one thread per parameter for the weight gradients
 // and the Adam update. Training targets are the kernels' own timings (soft targets favouring
@@ -26,14 +26,15 @@
 
 namespace rz {
 
-constexpr int kIn = 12, kH = 64, kOut = 49, kCfg = 48;
+constexpr int kIn = 12, kH = 64, kCfg = kConfigSpace, kOut = kCfg + 1;
+static_assert(kCfg >= 32 && kOut <= 64, "one warp holds the logits two per lane");
 constexpr int kOffW1 = 0;
 constexpr int kOffB1 = kOffW1 + kIn * kH;
 constexpr int kOffW2 = kOffB1 + kH;
 constexpr int kOffB2 = kOffW2 + kH * kH;
 constexpr int kOffW3 = kOffB2 + kH;
 constexpr int kOffB3 = kOffW3 + kH * kOut;
-constexpr int kParams = kOffB3 + kOut;  // 8177
+constexpr int kParams = kOffB3 + kOut;  // 8697
 constexpr int kSample = 4096;
 constexpr float kBitWeight = 0.5f;  // weight of the partition-bit loss
 
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(1024) features_kernel(const uint32_t* __restri
 }
 
 // ---- forward (+ loss gradient) ------------------------------------------------------------------
-// One warp per sample: lane l owns hidden units l and l+32 and outputs l, l+32 (< 49).
+// One warp per sample: lane l owns hidden units l and l+32 and outputs l, l+32 (< kOut).
 __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ X,
                                                           const float* __restrict__ Tg, const int* __restrict__ order,
                                                           int nsamp, float* __restrict__ H1, float* __restrict__ H2,
@@ -176,11 +177,11 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
     O[size_t(b) * kOut + lane] = o[0];
     if (lane + 32 < kOut) O[size_t(b) * kOut + lane + 32] = o[1];
     if (!Tg) return;
-    // Softmax cross-entropy over the 48 configuration logits (soft targets) + weighted binary
-    // cross-entropy of the partition bit (logit 48). Gradients are averaged over the batch.
+    // Softmax cross-entropy over the kCfg configuration logits (soft targets) + weighted binary
+    // cross-entropy of the partition bit (logit kCfg). Gradients are averaged over the batch.
     const float* t = Tg + size_t(src) * kOut;
-    const float l0 = o[0];                                        // unit lane (< 48 always)
-    const float l1 = (lane + 32 < kCfg) ? o[1] : -INFINITY;       // units 32..47
+    const float l0 = o[0];                                        // unit lane (< kCfg always)
+    const float l1 = (lane + 32 < kCfg) ? o[1] : -INFINITY;       // units 32..kCfg-1
     float mx = fmaxf(l0, l1);
     for (int d = 16; d > 0; d >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, d));
     const float e0 = __expf(l0 - mx), e1 = (lane + 32 < kCfg) ? __expf(l1 - mx) : 0.f;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
     const float inv = 1.f / float(nsamp);
     dO[size_t(b) * kOut + lane] = (e0 / se - t0) * inv;
     if (lane + 32 < kCfg) dO[size_t(b) * kOut + lane + 32] = (e1 / se - t1) * inv;
-    if (lane == 16) {  // unit 48: the partition bit
+    if (lane == kCfg - 32) {  // unit kCfg: the partition bit
         const float z = o[1];
         const float tb = __ldg(&t[kCfg]);
         const float pz = 1.f / (1.f + __expf(-z));
@@ -305,7 +306,7 @@ namespace rz {
 struct Predictor {
     rz_mlp* mlp = nullptr;
     float* d_feat = nullptr;  // 12 floats
-    float* d_out = nullptr;   // 49 floats
+    float* d_out = nullptr;   // kOut floats
 };
 
 static int ensure_batch(rz_mlp* m, size_t nsamp) {
@@ -469,7 +470,7 @@ int rz_mlp_features(rz_ctx* ctx, const uint32_t* d_idx, int64_t n, int64_t k, ui
     return RZ_OK;
 }
 
-// Forward pass over host features (nsamp x 12) -> host logits (nsamp x 49).
+// Forward pass over host features (nsamp x 12) -> host logits (nsamp x kOut).
 int rz_mlp_forward(rz_mlp* m, const float* h_x, int64_t nsamp, float* h_out) {
     if (!m || !h_x || !h_out || nsamp < 1) return RZ_ERR_INVALID_ARG;
     rz_ctx* ctx = m->ctx;
@@ -511,7 +512,7 @@ int rz_mlp_gradients(rz_mlp* m, const float* h_x, const float* h_t, int64_t nsam
     return st;
 }
 
-// Adam training on the GPU: nsamp samples (12 features, 49 targets each), mini-batches drawn by a
+// Adam training on the GPU: nsamp samples (12 features, kOut targets each), mini-batches drawn by a
 // seeded shuffle every epoch. *h_last_loss receives the mean loss of the last epoch.
 int rz_mlp_train(rz_mlp* m, const float* h_x, const float* h_t, int64_t nsamp, int32_t epochs, int32_t batch,
                  float lr, uint64_t seed, float* h_last_loss) {

@@ -6,7 +6,7 @@ Pipeline (``python -m redzone_b200.learn collect|train|eval``):
 * ``collect``: seeded removal instances drawn as mixes of the two single-list benchmark
   configurations (n = 2^20 and n = 2^28, plus intermediate sizes; int32 and 16-byte payloads;
   uniform, clustered and tail-heavy indices). For each: the 12 features from the GPU feature
-  kernel (``rz_mlp_features``) and the time of every one of the 48 launch configurations plus the
+  kernel (``rz_mlp_features``) and the time of every one of the 56 launch configurations plus the
   partition path (``rz_autotune_single``, CUDA events, L2 flushed between runs).
 * ``train``: soft targets (configurations within a few percent of the fastest get most of the
   mass) and the partition bit; Adam on the GPU through ``rz_mlp_train``.
@@ -32,7 +32,8 @@ import numpy as np
 from . import _native
 from ._native import LaunchCfg
 
-N_IN, N_OUT, N_CFG = 12, 49, 48
+N_IN, N_OUT, N_CFG = 12, 57, 56
+SCHED_AUTO, SCHED_CSCAN = 0, 4
 DATA = Path(__file__).resolve().parent / "data"
 _FP = ctypes.POINTER(ctypes.c_float)
 
@@ -41,9 +42,13 @@ def _fp(a: np.ndarray):
     return a.ctypes.data_as(_FP)
 
 
-def config_space() -> list[tuple[int, int, int]]:
-    """(block, items, grid scale) in the library's canonical order (class index = position)."""
-    return [(b, i, g) for b in (128, 256, 512, 1024) for i in (1, 2, 4, 8) for g in (1, 2, 4)]
+def config_space() -> list[tuple[int, int, int, int]]:
+    """(block, items, grid scale, schedule) in the library's canonical order (class index =
+    position): 48 points with the schedule chosen by k, then 8 cluster-scan launches."""
+    grid = [(b, i, g, SCHED_AUTO) for b in (128, 256, 512, 1024) for i in (1, 2, 4, 8) for g in (1, 2, 4)]
+    cscan = [(b, i, 2, SCHED_CSCAN) for b, i in ((128, 2), (128, 4), (256, 1), (256, 2), (256, 4), (256, 8),
+                                                  (512, 2), (512, 4))]
+    return grid + cscan
 
 
 class Mlp:
@@ -128,7 +133,7 @@ def attach_default(ctx) -> Mlp | None:
 
 # ---- training data ------------------------------------------------------------------------------
 def soft_targets(times: np.ndarray, tau: float = 0.03) -> np.ndarray:
-    """times: (N, 49) ms for the 48 configurations and the partition path -> (N, 49) targets."""
+    """times: (N, 57) ms for the 56 configurations and the partition path -> (N, 57) targets."""
     t = np.asarray(times, np.float64)
     cfg = t[:, :N_CFG]
     best = cfg.min(1, keepdims=True)
@@ -160,7 +165,7 @@ def draw_instance(rng: np.random.Generator) -> tuple[int, int, int, str]:
 
 
 def collect(ctx, count: int, seed: int, reps: int = 1, log_every: int = 500):
-    """Features and 49 timings for `count` seeded instances (timing rewrites a scratch array)."""
+    """Features and 57 timings for `count` seeded instances (timing rewrites a scratch array)."""
     import torch
     from . import workloads
 
@@ -188,7 +193,7 @@ def collect(ctx, count: int, seed: int, reps: int = 1, log_every: int = 500):
             if e.cfg.use_partition:
                 T[q, N_CFG] = e.ms
             else:
-                T[q, space[(e.cfg.block, e.cfg.items, e.cfg.ctas_per_sm)]] = e.ms
+                T[q, space[(e.cfg.block, e.cfg.items, e.cfg.ctas_per_sm, e.cfg.schedule)]] = e.ms
         X[q] = f
         meta[q] = (n, k, w, ["uniform", "clustered", "tail"].index(dist))
         if log_every and (q + 1) % log_every == 0:
@@ -201,12 +206,14 @@ def default_class(ctx, n, k, w) -> int:
     c = LaunchCfg()
     ctx._check(_native.lib.rz_default_cfg(ctx.handle, int(n), int(k), int(w), ctypes.byref(c)), "rz_default_cfg")
     space = config_space()
-    key = (c.block, c.items, c.ctas_per_sm)
+    key = (c.block, c.items, c.ctas_per_sm, c.schedule)
     if key in space:
         return space.index(key)
-    # The default's block may be clamped; pick the nearest class with the same items and grid.
-    return min(range(N_CFG), key=lambda q: (space[q][1] != c.items, space[q][2] != c.ctas_per_sm,
-                                            abs(space[q][0] - c.block)))
+    # The default's block may be clamped; pick the nearest class of the same schedule family with
+    # the same items and grid.
+    fam = SCHED_CSCAN if c.schedule == SCHED_CSCAN else SCHED_AUTO
+    return min(range(N_CFG), key=lambda q: (space[q][3] != fam, space[q][1] != c.items,
+                                            space[q][2] != c.ctas_per_sm, abs(space[q][0] - c.block)))
 
 
 def evaluate(pred_cls, pred_bit, T, default_cls) -> dict:

@@ -70,16 +70,16 @@ def test_feature_kernel_matches_cpu_oracle(ctx, dist, n, k, w):
 def test_training_on_the_gpu_learns_a_separable_task(ctx):
     rng = np.random.default_rng(0)
     x = rng.uniform(0, 1, (4000, 12)).astype(np.float32)
-    label = (x[:, 0] * 6).astype(int) * 8 + (x[:, 1] * 8).astype(int)  # 48 classes on a grid
-    t = np.zeros((4000, 49), np.float32)
+    label = (x[:, 0] * 7).astype(int) * 8 + (x[:, 1] * 8).astype(int)  # 56 classes on a grid
+    t = np.zeros((4000, mlp_ref.N_OUT), np.float32)
     t[np.arange(4000), label] = 1.0
-    t[:, 48] = (x[:, 2] > 0.5)
+    t[:, mlp_ref.N_CFG] = (x[:, 2] > 0.5)
     m = learn.Mlp(ctx, seed=2)
     before = m.gradients(x[:512], t[:512])[0]
     after = m.train(x, t, epochs=60, batch=256, lr=3e-3, seed=1)
     assert after < 0.5 * before
     cls, bit = m.predict(x)
-    assert np.mean(cls == label) > 0.8 and np.mean(bit == t[:, 48]) > 0.95
+    assert np.mean(cls == label) > 0.8 and np.mean(bit == t[:, mlp_ref.N_CFG]) > 0.95
     m.close()
 
 
@@ -135,7 +135,7 @@ def test_attached_predictor_is_used_and_falls_back(ctx):
             assert st == 0
             p = np.load(learn.DATA / "predictor.npz")["params"].astype(np.float64)
             _, _, o = mlp_ref.forward(p, mlp_ref.features(idx, n, k, 4)[None, :].astype(np.float64))
-            q = learn.config_space().index((cfg.block, cfg.items, cfg.ctas_per_sm))
+            q = learn.config_space().index((cfg.block, cfg.items, cfg.ctas_per_sm, cfg.schedule))
             assert o[0, q] >= o[0, : mlp_ref.N_CFG].max() - 1e-3  # the oracle's choice, up to a near-tie
         else:
             assert st == rz._native.RZ_ERR_UNSUPPORTED  # no network: rz_remove falls back to the tables

@@ -287,6 +287,16 @@ def test_cluster_scan_push_region_limit(ctx, red):
         assert np.array_equal(got[: n - k], exp[: n - k]), (red, cfg)
 
 
+def test_clobber_flag_is_accepted(ctx):
+    """RZ_CLOBBER_INDICES (the reference's contract: the removal list may be overwritten) is
+    accepted; the result is the canonical one and the list is still left as it was."""
+    n, k = 1 << 18, 1 << 13
+    host = payload(n, 1, seed=8)
+    idx = workloads.uniform(n, k, seed=8)
+    got = run_gpu(ctx, host, idx, flags=rz.RZ_SYNC | rz.RZ_CLOBBER_INDICES)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
 def test_cluster_scan_with_an_unaligned_index_list(ctx):
     """An index list that does not start on a 16-byte boundary runs on the grid schedule instead
     (the cluster scan reads it in 16-byte units), with the same result."""
