@@ -2,6 +2,7 @@
 // dispatch of single-list removals. Kernels live in rz_single.cu; batching, tuning, the learned
 // predictor and the service are in their own translation units.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -100,12 +101,35 @@ int map_status(uint32_t bits) {
 }
 
 // The status word (offset 0) and the device length (offset 512) of the workspace block come back
-// in one copy on the call's stream into pinned memory, then one stream synchronisation.
+// in one copy on the call's stream into pinned memory. The caller waits for it by polling an
+// event recorded after the copy, so a synchronous call returns within about a microsecond of
+// the copy landing; after kPollLimit of polling it blocks in cudaEventSynchronize instead.
 static constexpr size_t kResultBytes = 512 + sizeof(unsigned long long);
+static constexpr std::chrono::microseconds kPollLimit{2000};
+
+static int wait_event(rz_ctx* ctx, cudaEvent_t ev) {
+    const auto t0 = std::chrono::steady_clock::now();
+    bool polled = false;
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "cudaEventQuery");
+        polled = true;
+        if (std::chrono::steady_clock::now() - t0 > kPollLimit) {
+            RZ_CUDA_TRY(ctx, cudaEventSynchronize(ev));
+            break;
+        }
+    }
+    // "Not ready" is not a failure: do not leave it behind as the thread's last error.
+    if (polled && cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+    return RZ_OK;
+}
 
 static int fetch_result(rz_ctx* ctx, cudaStream_t s, uint32_t* status, unsigned long long* len) {
     RZ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ws.h_result, ctx->ws.status, kResultBytes, cudaMemcpyDeviceToHost, s));
-    RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    RZ_CUDA_TRY(ctx, cudaEventRecord(ctx->done_event, s));
+    const int st = wait_event(ctx, ctx->done_event);
+    if (st != RZ_OK) return st;
     std::memcpy(status, ctx->ws.h_result, sizeof(uint32_t));
     if (len) std::memcpy(len, ctx->ws.h_result + 512, sizeof(unsigned long long));
     return RZ_OK;
@@ -194,6 +218,14 @@ int rz_create(rz_ctx** out, int device) {
         return st;
     }
     w.h_result = static_cast<uint8_t*>(hr);
+    e = cudaEventCreateWithFlags(&ctx->done_event, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        int st = cuda_fail(ctx, e, "completion event");
+        cudaFreeHost(hr);
+        cudaFree(p);
+        delete ctx;
+        return st;
+    }
     *out = ctx;
     return RZ_OK;
 }
@@ -205,6 +237,7 @@ void rz_destroy(rz_ctx* ctx) {
     Workspace& w = ctx->ws;
     cudaFree(w.status);
     if (w.h_result) cudaFreeHost(w.h_result);
+    if (ctx->done_event) cudaEventDestroy(ctx->done_event);
     cudaFree(w.bitmap);
     cudaFree(w.dlist);
     cudaFree(w.slist);

@@ -70,6 +70,7 @@ struct rz_ctx {
     void* tune_table = nullptr;  // rz::TuneTable*, owned (see rz_autotune.cpp)
     size_t scratch_held = 0;     // bytes of grown context scratch
     size_t scratch_limit = ~size_t(0);  // rz_set_scratch_limit: growth beyond it -> RZ_ERR_NO_MEMORY
+    cudaEvent_t done_event = nullptr;    // completion of a synchronous call's last copy (polled)
 };
 
 namespace rz {
