@@ -168,6 +168,52 @@ int rz_remove_by_key(rz_ctx* ctx, rz_keyindex* ix, void* d_data, int64_t n, uint
                      const uint64_t* d_keys, int64_t k, int64_t* new_len, uint32_t flags, rz_stream_t stream);
 
 /*
+ * Removal lists made on the GPU, with the red-zone marking fused into the producer (the paper's
+ * "mark during producer" optimisation, p.14; no counterpart in the reference's code, whose
+ * phase 1, redzone.hxx:698-707, scans the finished list). A caller's kernel that decides which
+ * rows to delete calls rz_emit (include/redzone_device.cuh) for each of them; rz_emit appends the
+ * row to the producer's list and, when the row could fall in the red zone [n - k, n) (it is
+ * >= n - capacity), also to a short candidate list of (slot, row) pairs. rz_remove_produced then
+ * removes the emitted rows with the canonical rule; every CTA learns the red entries from the
+ * candidates, so no CTA scans the whole list and none waits for another, and k never has to
+ * reach the host.
+ *   rz_producer_create  -- capacity: most rows one round may emit (<= 2^18); cand_capacity:
+ *                          candidate slots (about capacity^2 / n + margin; when exceeded, the
+ *                          removal falls back to reading the list itself, still exact).
+ *   rz_producer_reset   -- start a round for a list of n rows (n < 2^32): zeroes the counts on
+ *                          `stream`. Take the view after each reset.
+ *   rz_producer_get_view -- the plain struct a producer kernel passes to rz_emit.
+ *   rz_remove_produced  -- remove the rows emitted since the reset from d_data[0..n), asynchronous;
+ *                          the new length n - k is on the device (counts[0] gives k) and, with
+ *                          RZ_SYNC, in *new_len. A round that emitted more than `capacity` rows
+ *                          fails with RZ_ERR_NO_MEMORY and moves nothing. RZ_VALIDATE reads k back
+ *                          (one synchronisation) and checks the list first.
+ *   rz_produce_where_less -- a producer provided by the library: emits every row i < n with
+ *                          d_keys[i] < threshold.
+ *   rz_producer_download -- synchronous copy of the round's list to the host (up to max entries);
+ *                          *k and *candidates receive the counts.
+ */
+typedef struct rz_producer_view {
+    uint32_t* idx;            /* the removal list, capacity entries                               */
+    uint32_t* counts;         /* [0] rows emitted (k), [1] candidates emitted                     */
+    uint32_t* cand;           /* candidates: (slot in idx, row) pairs, cand_capacity of them       */
+    uint32_t capacity;
+    uint32_t cand_capacity;
+    uint32_t n;               /* length of the list the round removes from                        */
+    uint32_t floor;           /* max(0, n - capacity): rows >= floor are candidates                */
+} rz_producer_view;
+typedef struct rz_producer rz_producer;
+int rz_producer_create(rz_ctx* ctx, int64_t capacity, int64_t cand_capacity, rz_producer** out);
+void rz_producer_destroy(rz_producer* p);
+int rz_producer_reset(rz_producer* p, int64_t n, rz_stream_t stream);
+int rz_producer_get_view(const rz_producer* p, rz_producer_view* out);
+int rz_remove_produced(rz_ctx* ctx, rz_producer* p, void* d_data, uint32_t elem_bytes, int64_t* new_len,
+                       uint32_t flags, rz_stream_t stream);
+int rz_produce_where_less(rz_producer* p, const uint32_t* d_keys, uint32_t threshold, rz_stream_t stream);
+int rz_producer_download(const rz_producer* p, uint32_t* h_idx, int64_t max, int64_t* k, int64_t* candidates,
+                         rz_stream_t stream);
+
+/*
  * O(n) stable partition comparator (mark, per-tile counts and their scan, then a pipelined
  * in-place move), in place. Survivors keep their relative order, as with thrust::remove
  * (Thrust_remove.hxx:15-17) and InK compact (cuCompactor.cuh:104-141).

@@ -296,6 +296,64 @@ class KeyIndex:
             pass
 
 
+class Producer:
+    """A removal list made on the GPU with the red-zone marking fused into its producer
+    (rz_producer_*; the device side is rz_emit in include/redzone_device.cuh)."""
+
+    def __init__(self, ctx: Context, capacity: int, cand_capacity: int = 4096):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx._check(_native.lib.rz_producer_create(ctx.handle, int(capacity), int(cand_capacity), ctypes.byref(h)),
+                   "rz_producer_create")
+        self.handle = h
+
+    def reset(self, n: int, stream=None) -> None:
+        """Start a round for a list of n rows (zeroes the counts on the stream)."""
+        self.ctx._check(_native.lib.rz_producer_reset(self.handle, int(n), ctypes.c_void_p(_stream_handle(stream))),
+                        "rz_producer_reset")
+
+    def view(self):
+        v = _native.ProducerView()
+        self.ctx._check(_native.lib.rz_producer_get_view(self.handle, ctypes.byref(v)), "rz_producer_get_view")
+        return v
+
+    def produce_where_less(self, keys, threshold: int, stream=None) -> None:
+        """Emit every row i with keys[i] < threshold (keys: CUDA uint32/int32 tensor of n entries)."""
+        self.ctx._check(_native.lib.rz_produce_where_less(self.handle, ctypes.c_void_p(keys.data_ptr()),
+                                                          int(threshold), ctypes.c_void_p(_stream_handle(stream))),
+                        "rz_produce_where_less")
+
+    def download(self, stream=None):
+        """(list as a numpy uint32 array, k, candidates emitted); synchronous."""
+        import numpy as np
+        v = self.view()
+        buf = np.zeros(max(1, v.capacity), np.uint32)
+        k, c = ctypes.c_int64(0), ctypes.c_int64(0)
+        self.ctx._check(_native.lib.rz_producer_download(self.handle, buf.ctypes.data, buf.size, ctypes.byref(k),
+                                                         ctypes.byref(c), ctypes.c_void_p(_stream_handle(stream))),
+                        "rz_producer_download")
+        return buf[: min(k.value, v.capacity)].copy(), k.value, c.value
+
+    def remove(self, data, flags: int = 0, stream=None) -> int:
+        """Remove the emitted rows from data[0..n); returns n - k with RZ_SYNC, else -1."""
+        out = ctypes.c_int64(0)
+        self.ctx._check(_native.lib.rz_remove_produced(self.ctx.handle, self.handle, ctypes.c_void_p(data.data_ptr()),
+                                                       item_bytes(data), ctypes.byref(out), flags,
+                                                       ctypes.c_void_p(_stream_handle(stream))), "rz_remove_produced")
+        return out.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _native.lib.rz_producer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Service:
     """Streaming delete service over a device-resident table (rz_service_*).
 

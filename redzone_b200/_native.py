@@ -68,6 +68,11 @@ class TuneEntry(ctypes.Structure):
     _fields_ = [("cfg", LaunchCfg), ("ms", c_f32)]
 
 
+class ProducerView(ctypes.Structure):
+    _fields_ = [("idx", c_vp), ("counts", c_vp), ("cand", c_vp), ("capacity", c_u32), ("cand_capacity", c_u32),
+                ("n", c_u32), ("floor", c_u32)]
+
+
 def _sig(name, restype, argtypes):
     f = getattr(lib, name)
     f.restype = restype
@@ -100,6 +105,13 @@ _sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchC
 _sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
 _sig("rz_last_launch", c_i32, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)])
 _sig("rz_remove_noalloc", c_i32, [c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_vp])
+_sig("rz_producer_create", c_i32, [c_vp, c_i64, c_i64, ctypes.POINTER(c_vp)])
+_sig("rz_producer_destroy", None, [c_vp])
+_sig("rz_producer_reset", c_i32, [c_vp, c_i64, c_vp])
+_sig("rz_producer_get_view", c_i32, [c_vp, ctypes.POINTER(ProducerView)])
+_sig("rz_remove_produced", c_i32, [c_vp, c_vp, c_vp, c_u32, ctypes.POINTER(c_i64), c_u32, c_vp])
+_sig("rz_produce_where_less", c_i32, [c_vp, c_vp, c_u32, c_vp])
+_sig("rz_producer_download", c_i32, [c_vp, c_vp, c_i64, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64), c_vp])
 _sig("rz_batch_plan_create", c_i32, [c_vp, ctypes.POINTER(ListDesc), c_i32, c_u32, ctypes.POINTER(BatchCfg),
                                      ctypes.POINTER(c_vp)])
 _sig("rz_batch_plan_launch", c_i32, [c_vp, c_vp])

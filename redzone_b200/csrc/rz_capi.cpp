@@ -93,6 +93,7 @@ int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {
 }
 
 int map_status(uint32_t bits) {
+    if (bits & 16u) return RZ_ERR_NO_MEMORY;
     if (bits & 2u) return RZ_ERR_OUT_OF_RANGE;
     if (bits & 1u) return RZ_ERR_DUPLICATE;
     if (bits & 4u) return RZ_ERR_TIMEOUT;
@@ -135,10 +136,12 @@ static int fetch_result(rz_ctx* ctx, cudaStream_t s, uint32_t* status, unsigned 
     return RZ_OK;
 }
 
-int read_status(rz_ctx* ctx, cudaStream_t s) {
+int read_status(rz_ctx* ctx, cudaStream_t s, int64_t* new_len) {
     uint32_t h = 0;
-    int st = fetch_result(ctx, s, &h, nullptr);
+    unsigned long long dl = 0;
+    int st = fetch_result(ctx, s, &h, new_len ? &dl : nullptr);
     if (st != RZ_OK) return st;
+    if (new_len) *new_len = int64_t(dl);
     if (h) {
         RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
         // A failed call may have left barrier state or bitmap bits behind.

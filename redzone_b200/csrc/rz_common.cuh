@@ -19,6 +19,7 @@ enum : uint32_t {
     ST_RANGE = 1u << 1,
     ST_TIMEOUT = 1u << 2,
     ST_INCONSISTENT = 1u << 3,  // orphan counts disagree (only possible with invalid input)
+    ST_CAPACITY = 1u << 4,      // a produced list outgrew its capacity (nothing was moved)
 };
 
 // 32-byte payload (u64 key + three u64 words in the streaming table; 8 x u32 otherwise).

@@ -29,6 +29,7 @@
 
 #include "rz_common.cuh"
 #include "rz_internal.h"
+#include "rz_pairfill.cuh"
 #include "rz_single_kernel.cuh"
 
 namespace cg = cooperative_groups;
@@ -51,12 +52,12 @@ struct CscanParams {
     uint32_t validate;
 };
 
-// Dynamic shared memory: full V and P maps, this slice's V and P maps, per-word prefix arrays of
-// the slow path (six k-bit-map-sized arrays), red positions / values / source orphans
-// (kFastMaxRed words each) and the Q push regions (kCscanRegCap uint2 each).
+// Dynamic shared memory: the pairing layout of rz_pairfill.cuh (full V and P maps, the slow
+// path's two prefix arrays, red positions / values / source orphans), then this slice's V and P
+// maps and the Q push regions (kCscanRegCap uint2 each).
 __host__ __device__ inline size_t cscan_smem_bytes(uint32_t k) {
     const size_t kw = (k + 31) / 32;
-    return (6 * kw + 3 * size_t(kFastMaxRed)) * 4 + size_t(kCscanQ) * kCscanRegCap * 8;
+    return (pairfill_words(uint32_t(kw)) + 2 * kw) * 4 + size_t(kCscanQ) * kCscanRegCap * 8;
 }
 
 __device__ __forceinline__ void cluster_arrive() {
@@ -133,18 +134,16 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
     const uint32_t lt = lanemask_lt();
 
     extern __shared__ __align__(16) uint32_t s_dyn[];
-    uint32_t* mapV = s_dyn;
-    uint32_t* mapP = mapV + kw;
-    uint32_t* pV = mapP + kw;   // this slice's red entries only (read by the cluster: slow path)
-    uint32_t* pP = pV + kw;
-    uint32_t* s_dpre = pP + kw;  // slow path: per-word prefix of destination orphans
-    uint32_t* s_spre = s_dpre + kw;  // slow path: per-word prefix of source orphans
-    uint32_t* s_pos = s_spre + kw;
-    uint32_t* s_val = s_pos + kFastMaxRed;
-    uint32_t* s_src = s_val + kFastMaxRed;
-    uint2* s_reg = reinterpret_cast<uint2*>(s_src + kFastMaxRed);  // push region r: [r * cap, +cap)
     __shared__ uint32_t s_cnt[2][16 * 16 + 1];
     __shared__ uint32_t s_scan[33];
+    const PairFillSmem pf{s_dyn, kw, s_cnt, s_scan};
+    uint32_t* mapV = pf.mapV();
+    uint32_t* mapP = pf.mapP();
+    uint32_t* s_pos = pf.pos();
+    uint32_t* s_val = pf.val();
+    uint32_t* pV = s_dyn + pairfill_words(kw);  // this slice's red entries only (read by the cluster: slow path)
+    uint32_t* pP = pV + kw;
+    uint2* s_reg = reinterpret_cast<uint2*>(pP + kw);  // push region r: [r * cap, +cap)
     __shared__ uint32_t s_qcnt[kCscanQ];     // pushed: red entries of each rank's slice
     __shared__ uint32_t s_qc[kCscanQ + 1];   // their prefix
     __shared__ uint32_t s_total;
@@ -164,7 +163,12 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
             src[j] = tail[i];
         }
     }
-    for (uint32_t w = threadIdx.x; w < kw; w += B) reinterpret_cast<uint4*>(s_dyn)[w] = make_uint4(0u, 0u, 0u, 0u);  // all four maps
+    for (uint32_t w = threadIdx.x; w < kw; w += B) {  // the four maps
+        mapV[w] = 0u;
+        mapP[w] = 0u;
+        pV[w] = 0u;
+        pP[w] = 0u;
+    }
     __syncthreads();  // s_abort, zeroed maps
     if (s_abort) {
         // Validation failed: leave the caller's data untouched. Every CTA still passes the same
@@ -279,180 +283,12 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
     __syncthreads();
     CS_STAMP(6);
 
-    uint32_t stot = 0;  // source orphans of the whole list
-    uint32_t dbase = 0;  // destination orphans before this tile (fast path)
-    uint32_t* cbuf = s_cnt[1];
-    if (fast && R <= 32u && E <= 32) {
-        // Few red entries (the usual case: about k^2/n of them): warp 0 pairs them, one lane per
-        // entry, while another warp scans this tile's V \ P word counts; one barrier.
-        if (warp == 0) {
-            uint32_t ps = 0;
-            bool sf = false, af = false, df = false;
-            if (uint32_t(lane) < R) {
-                ps = s_pos[lane];
-                const uint32_t v = s_val[lane];
-                sf = !((mapV[ps >> 5] >> (ps & 31u)) & 1u);
-                af = !((mapP[v >> 5] >> (v & 31u)) & 1u);
-                df = af && v < chunk_base;
-            }
-            const uint32_t bs = __ballot_sync(0xffffffffu, sf);
-            const uint32_t bd = __ballot_sync(0xffffffffu, df);
-            const uint32_t ba = __ballot_sync(0xffffffffu, af);
-            if (sf) s_src[__popc(bs & lt)] = ps;
-            if (lane == 0) {
-                s_scan[0] = __popc(bs);
-                s_scan[1] = __popc(bd);
-                if (blockIdx.x == 0 && __popc(ba) != __popc(bs)) atomicOr(p.status, ST_INCONSISTENT);
-            }
-        }
-        if (warp == (nw > 1 ? 1 : 0)) {
-            // cbuf[j * nw + w] = V \ P bits of this tile before word (j, w), then cbuf[E] = all.
-            uint32_t x = 0;
-            if (lane < E) {
-                const uint32_t i0 = chunk_base + uint32_t(lane / nw) * B + uint32_t(lane % nw) * 32u;
-                x = (t < ntiles && i0 < k) ? __popc(mapV[i0 >> 5] & ~mapP[i0 >> 5]) : 0u;
-            }
-            const uint32_t inc = warp_inclusive_scan(x);
-            if (lane < E) cbuf[lane] = inc - x;
-        }
-        __syncthreads();
-        stot = s_scan[0];
-        dbase = s_scan[1];
-    } else if (fast) {
-        // Ranks inside this tile: one word of the V \ P map per (round, warp).
-        if (lane == 0) {
-#pragma unroll
-            for (int j = 0; j < IPT; ++j) {
-                const uint32_t i0 = chunk_base + uint32_t(j) * B + uint32_t(warp) * 32u;
-                cbuf[j * nw + warp] = (t < ntiles && i0 < k) ? __popc(mapV[i0 >> 5] & ~mapP[i0 >> 5]) : 0u;
-            }
-        }
-        // Source orphans compacted in position order; destination orphans before this tile and
-        // in all: rounds of B red entries, per-warp ballot counts, one barrier per round.
-        uint32_t dall = 0;
-        for (uint32_t q0 = 0, rd = 0; q0 == 0 || q0 < R; q0 += B, ++rd) {
-            uint32_t* wc = s_cnt[0] + 96u * (rd & 1u);
-            const uint32_t e = q0 + threadIdx.x;
-            uint32_t ps = 0;
-            bool sf = false, af = false, df = false;
-            if (e < R) {
-                ps = s_pos[e];
-                const uint32_t v = s_val[e];
-                sf = !((mapV[ps >> 5] >> (ps & 31u)) & 1u);
-                af = !((mapP[v >> 5] >> (v & 31u)) & 1u);
-                df = af && v < chunk_base;
-            }
-            const uint32_t bs = __ballot_sync(0xffffffffu, sf);
-            const uint32_t bd = __ballot_sync(0xffffffffu, df);
-            const uint32_t ba = __ballot_sync(0xffffffffu, af);
-            if (lane == 0) {
-                wc[warp] = __popc(bs);
-                wc[32 + warp] = __popc(bd);
-                wc[64 + warp] = __popc(ba);
-            }
-            __syncthreads();
-            uint32_t pre = 0, ts = 0;
-            for (int w2 = 0; w2 < nw; ++w2) {
-                const uint32_t x = wc[w2];
-                pre += w2 < warp ? x : 0u;
-                ts += x;
-                dbase += wc[32 + w2];
-                dall += wc[64 + w2];
-            }
-            if (sf) s_src[stot + pre + __popc(bs & lt)] = ps;
-            stot += ts;
-        }
-        if (threadIdx.x == 0 && blockIdx.x == 0 && dall != stot) atomicOr(p.status, ST_INCONSISTENT);
-        if (warp == 0) warp0_scan_counts(cbuf, E, lane);
-        __syncthreads();
-    } else {
-        // Per-word prefixes of destination (V & ~P) and source (P & ~V) orphans, in word order:
-        // warp w owns a contiguous block of words, lane l reads word j * 32 + l of it.
-        const uint32_t per = (kw + B - 1) / B;
-        const uint32_t wb = uint32_t(warp) * 32u * per;
-        uint32_t ssum = 0, dsum = 0;  // counts can reach k here: summed separately, not packed
-        for (uint32_t j = 0; j < per; ++j) {
-            const uint32_t w = wb + j * 32u + uint32_t(lane);
-            if (w < kw) {
-                const uint32_t v = mapV[w], pm = mapP[w];
-                ssum += uint32_t(__popc(pm & ~v));
-                dsum += uint32_t(__popc(v & ~pm));
-            }
-        }
-        ssum = warp_inclusive_scan(ssum);
-        dsum = warp_inclusive_scan(dsum);
-        if (lane == 31) {
-            s_cnt[0][warp] = ssum;
-            s_cnt[0][32 + warp] = dsum;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t xs = lane < nw ? s_cnt[0][lane] : 0u, xd = lane < nw ? s_cnt[0][32 + lane] : 0u;
-            const uint32_t is = warp_inclusive_scan(xs), id = warp_inclusive_scan(xd);
-            if (lane < nw) {
-                s_cnt[0][64 + lane] = is - xs;
-                s_cnt[0][96 + lane] = id - xd;
-            }
-            if (lane == 31) {
-                s_cnt[0][128] = is;
-                s_cnt[0][129] = id;
-            }
-        }
-        __syncthreads();
-        uint32_t cs = s_cnt[0][64 + warp], cd = s_cnt[0][96 + warp];
-        for (uint32_t j = 0; j < per; ++j) {
-            const uint32_t w = wb + j * 32u + uint32_t(lane);
-            uint32_t v = 0, pm = 0;
-            if (w < kw) {
-                v = mapV[w];
-                pm = mapP[w];
-            }
-            const uint32_t xs = uint32_t(__popc(pm & ~v)), xd = uint32_t(__popc(v & ~pm));
-            const uint32_t is = warp_inclusive_scan(xs), id = warp_inclusive_scan(xd);
-            if (w < kw) {
-                s_spre[w] = cs + is - xs;
-                s_dpre[w] = cd + id - xd;
-            }
-            cs += __shfl_sync(0xffffffffu, is, 31);
-            cd += __shfl_sync(0xffffffffu, id, 31);
-        }
-        stot = s_cnt[0][128];
-        if (threadIdx.x == 0 && blockIdx.x == 0 && s_cnt[0][129] != stot) atomicOr(p.status, ST_INCONSISTENT);
-        __syncthreads();
-    }
+    uint32_t stot, dbase;
+    derive_pairing<IPT>(pf, R, k, chunk_base, t < ntiles, p.status, stot, dbase);
     CS_STAMP(3);
 
     // ---- this tile: fill holes, pair destination orphans ---------------------------------------
-    if (t < ntiles) {
-#pragma unroll
-        for (int j = 0; j < IPT; ++j) {
-            const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
-            if (i >= k || rr[j] >= cut) continue;  // past the list, or a hole needing no fill
-            const uint32_t vw = mapV[i >> 5];
-            if (!((vw >> lane) & 1u)) {
-                head[rr[j]] = src[j];  // valid source, valid destination
-                continue;
-            }
-            const uint32_t below = __popc(vw & ~mapP[i >> 5] & lt);
-            const uint32_t rank = fast ? dbase + cbuf[j * nw + warp] + below : s_dpre[i >> 5] + below;
-            if (rank >= stot) continue;  // only with invalid input (reported above)
-            uint32_t spos;
-            if (fast) {
-                spos = s_src[rank];
-            } else {
-                // The word holding the rank-th source orphan: last word whose prefix <= rank.
-                uint32_t lo = 0, hi = kw;
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (s_spre[mid] <= rank) lo = mid; else hi = mid;
-                }
-                uint32_t sw = mapP[lo] & ~mapV[lo];
-                for (uint32_t c = rank - s_spre[lo]; c > 0u; --c) sw &= sw - 1u;  // drop lower ones
-                spos = lo * 32u + uint32_t(__ffs(sw) - 1);
-            }
-            head[rr[j]] = tail[spos];
-        }
-    }
+    if (t < ntiles) fill_holes<W, IPT>(pf, R, k, cut, chunk_base, stot, dbase, rr, src, head, tail);
     CS_STAMP(4);
     cluster_wait();  // phase 2: no CTA leaves while another may still read its shared memory
     if (blockIdx.x == 0 && threadIdx.x == 0 && p.dev_len) *p.dev_len = (unsigned long long)(n - k);

@@ -136,7 +136,9 @@ bool predict_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, const uint32_t
                  cudaStream_t s, rz_launch_cfg* cfg);
 bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
 void release_extras(rz_ctx* ctx);
-int read_status(rz_ctx* ctx, cudaStream_t s);
+// Wait for the stream, then map the device status to rz_status (clearing it); with new_len, also
+// read back the device-tracked length of the last call.
+int read_status(rz_ctx* ctx, cudaStream_t s, int64_t* new_len = nullptr);
 
 // Batched launches into preallocated scratch (rz_batched.cu), for the streaming service.
 struct BatchArena;

@@ -1,0 +1,398 @@
+// rz_produced.cu -- removal of a list made on the GPU, with the red-zone marking fused into its
+// producer (the paper's "mark during producer", p.14). No counterpart in the reference's code:
+// there, phase 1 (redzone.hxx:698-707) scans the finished list for entries >= n - k.
+//
+// The producer (rz_emit, include/redzone_device.cuh) appends each deleted row to a list and,
+// when the row is >= n - capacity, also to a candidate list of (slot, row) pairs. Every red entry
+// (idx[i] >= n - k, with k <= capacity) is among the candidates, so a CTA of the removal learns
+// all red entries by reading the candidates -- typically a few dozen pairs -- instead of its
+// share of a k-entry list plus an exchange with the other CTAs. The removal kernel therefore has
+// no barrier of any kind between CTAs: each CTA reads its tile (index and tail item) and the
+// candidates at once, builds the V and P maps in shared memory, orders the red entries by
+// position and derives the canonical pairing exactly as the cluster-scan schedule does
+// (rz_pairfill.cuh). k itself is read on the device: the host never waits for the producer.
+// If the candidates overflowed their buffer, each CTA reads the whole list instead (exact,
+// slower); if the list outgrew its capacity, nothing moves and the status says so.
+#include <algorithm>
+#include <atomic>
+#include <new>
+
+#include "../../include/redzone_device.cuh"
+#include "rz_common.cuh"
+#include "rz_internal.h"
+#include "rz_pairfill.cuh"
+
+struct rz_producer {
+    rz_ctx* ctx = nullptr;
+    uint32_t* idx = nullptr;
+    uint32_t* counts = nullptr;  // [0] rows, [1] candidates (own 256-byte block)
+    uint32_t* cand = nullptr;    // (slot, row) pairs
+    uint32_t capacity = 0;
+    uint32_t cand_capacity = 0;
+    uint32_t n = 0;
+    bool have_n = false;
+};
+
+namespace rz {
+
+constexpr uint32_t kProducedMaxK = 1u << 18;  // list capacity: four k-bit maps in shared memory
+constexpr int kProducedBlock = 256;
+
+// Dynamic shared memory for a list of at most `capacity` rows: V and P maps and the two prefix
+// arrays of the slow path (capacity bits each), then ordered red positions / values, source
+// orphans, and the unordered red entries as collected (kFastMaxRed words each).
+static size_t produced_smem_bytes(uint32_t capacity) {
+    return (pairfill_words((capacity + 31) / 32) + 2 * size_t(kFastMaxRed)) * 4;
+}
+
+struct ProducedParams {
+    uint8_t* data;
+    const uint32_t* idx;
+    const uint32_t* counts;
+    const uint2* cand;
+    uint32_t n, capacity, cand_capacity;
+    uint32_t* status;
+    unsigned long long* dev_len;
+    uint32_t validate;
+};
+
+template <int W, int IPT>
+__global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(const ProducedParams p) {
+    using T = typename Payload<W>::T;
+    const uint32_t k = __ldcg(&p.counts[0]), m = __ldcg(&p.counts[1]);
+    const uint32_t n = p.n;
+    if (k > p.capacity) {  // uniform: every CTA reads the same counts
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.status, ST_CAPACITY);
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && p.dev_len) *p.dev_len = (unsigned long long)(n - k);
+    const uint32_t B = blockDim.x, TILE = B * IPT;
+    const uint32_t ntiles = (k + TILE - 1) / TILE;
+    const uint32_t t = blockIdx.x;
+    if (t >= ntiles || k == n) return;  // no tile here, or nothing survives (nothing moves)
+    const uint32_t cut = n - k, kw = (k + 31) >> 5, kwc = (p.capacity + 31) >> 5;
+    const uint32_t chunk_base = t * TILE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = int(B >> 5);
+    T* __restrict__ head = reinterpret_cast<T*>(p.data);
+    const T* __restrict__ tail = reinterpret_cast<const T*>(p.data) + cut;
+
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    __shared__ uint32_t s_cnt[2][16 * 16 + 1];
+    __shared__ uint32_t s_scan[33];
+    const PairFillSmem pf{s_dyn, kwc, s_cnt, s_scan};
+    uint32_t* mapV = pf.mapV();
+    uint32_t* mapP = pf.mapP();
+    uint32_t* s_spre = pf.spre();
+    uint32_t* s_pos = pf.pos();
+    uint32_t* s_val = pf.val();
+    uint32_t* u_pos = s_dyn + pairfill_words(kwc);  // red entries as collected (any order)
+    uint32_t* u_val = u_pos + kFastMaxRed;
+    __shared__ uint32_t s_R;
+    __shared__ int s_abort;
+
+    if (threadIdx.x == 0) {
+        s_R = 0;
+        s_abort = p.validate ? ((__ldcg(p.status) & (ST_DUPLICATE | ST_RANGE)) != 0) : 0;
+    }
+    uint32_t rr[IPT];
+    T src[IPT];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+        const uint32_t i = chunk_base + uint32_t(j) * B + threadIdx.x;
+        rr[j] = 0xffffffffu;
+        if (i < k) {
+            rr[j] = __ldcg(&p.idx[i]);
+            src[j] = tail[i];
+        }
+    }
+    for (uint32_t w = threadIdx.x; w < kw; w += B) {
+        mapV[w] = 0u;
+        mapP[w] = 0u;
+    }
+    __syncthreads();
+    if (s_abort) return;  // validation failed: nothing moves
+
+    // ---- the red entries: from the candidates, or (candidates overflowed) from the whole list ---
+    const bool from_cand = m <= p.cand_capacity;
+    const uint32_t scan_n = from_cand ? m : k;
+    for (uint32_t e = threadIdx.x; e < scan_n; e += B) {
+        uint32_t slot, row;
+        if (from_cand) {
+            const uint2 c = __ldcg(&p.cand[e]);
+            slot = c.x;
+            row = c.y;
+        } else {
+            slot = e;
+            row = __ldcg(&p.idx[e]);
+        }
+        if (row >= n) {
+            atomicOr(p.status, ST_RANGE);
+            continue;
+        }
+        if (row < cut || slot >= k) continue;
+        const uint32_t v = row - cut;
+        atomicOr(&mapV[v >> 5], 1u << (v & 31u));
+        atomicOr(&mapP[slot >> 5], 1u << (slot & 31u));
+        const uint32_t r = atomicAdd(&s_R, 1u);
+        if (r < kFastMaxRed) {
+            u_pos[r] = slot;
+            u_val[r] = v;
+        }
+    }
+    __syncthreads();
+    const uint32_t R = s_R > kFastMaxRed ? 0xffffffffu : s_R;
+
+    // ---- red entries in position order ----------------------------------------------------------
+    if (R <= 32u) {
+        if (warp == 0) {
+            const uint32_t ps = uint32_t(lane) < R ? u_pos[lane] : 0xffffffffu;
+            uint32_t rank = 0;
+            for (uint32_t d = 0; d < R; ++d) rank += __shfl_sync(0xffffffffu, ps, int(d)) < ps ? 1u : 0u;
+            if (uint32_t(lane) < R) {
+                s_pos[rank] = ps;
+                s_val[rank] = u_val[lane];
+            }
+        }
+    } else if (R <= kFastMaxRed) {
+        // rank(slot) = set bits of P before it: per-word prefix of the P map (into s_spre, which
+        // only the slow path uses otherwise), warp w owning a contiguous block of words.
+        const uint32_t per = (kw + B - 1) / B;
+        const uint32_t wb = uint32_t(warp) * 32u * per;
+        uint32_t sum = 0;
+        for (uint32_t j = 0; j < per; ++j) {
+            const uint32_t w = wb + j * 32u + uint32_t(lane);
+            if (w < kw) sum += uint32_t(__popc(mapP[w]));
+        }
+        sum = warp_inclusive_scan(sum);
+        if (lane == 31) s_cnt[0][warp] = sum;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t x = lane < nw ? s_cnt[0][lane] : 0u;
+            const uint32_t inc = warp_inclusive_scan(x);
+            if (lane < nw) s_cnt[0][32 + lane] = inc - x;
+        }
+        __syncthreads();
+        uint32_t run = s_cnt[0][32 + warp];
+        for (uint32_t j = 0; j < per; ++j) {
+            const uint32_t w = wb + j * 32u + uint32_t(lane);
+            const uint32_t x = w < kw ? uint32_t(__popc(mapP[w])) : 0u;
+            const uint32_t inc = warp_inclusive_scan(x);
+            if (w < kw) s_spre[w] = run + inc - x;
+            run += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < R; e += B) {
+            const uint32_t ps = u_pos[e];
+            const uint32_t rank = s_spre[ps >> 5] + uint32_t(__popc(mapP[ps >> 5] & ((1u << (ps & 31u)) - 1u)));
+            s_pos[rank] = ps;
+            s_val[rank] = u_val[e];
+        }
+    }
+    __syncthreads();
+
+    uint32_t stot, dbase;
+    derive_pairing<IPT>(pf, R, k, chunk_base, true, p.status, stot, dbase);
+    fill_holes<W, IPT>(pf, R, k, cut, chunk_base, stot, dbase, rr, src, head, tail);
+}
+
+using ProducedFn = void (*)(const ProducedParams);
+
+template <int W>
+static ProducedFn produced_fn(int items) {
+    switch (items) {
+        case 1: return redzone_produced_kernel<W, 1>;
+        case 2: return redzone_produced_kernel<W, 2>;
+        case 4: return redzone_produced_kernel<W, 4>;
+        case 8: return redzone_produced_kernel<W, 8>;
+        default: return nullptr;
+    }
+}
+static ProducedFn produced_fn(uint32_t w, int items) {
+    switch (w) {
+        case 4: return produced_fn<4>(items);
+        case 8: return produced_fn<8>(items);
+        case 16: return produced_fn<16>(items);
+        case 32: return produced_fn<32>(items);
+        default: return nullptr;
+    }
+}
+
+// The library's own producer: every row i < n with keys[i] < threshold.
+__global__ void produce_where_less_kernel(const rz_producer_view v, const uint32_t* __restrict__ keys,
+                                          uint32_t threshold) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    // Every lane of a warp runs the same number of iterations (rz_emit is called warp-wide).
+    const uint64_t n_round = (uint64_t(v.n) + 31u) & ~uint64_t(31);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        const bool take = i < v.n && __ldg(&keys[i]) < threshold;
+        rz_emit(v, uint32_t(i), take);
+    }
+}
+
+}  // namespace rz
+
+using namespace rz;
+
+extern "C" {
+
+int rz_producer_create(rz_ctx* ctx, int64_t capacity, int64_t cand_capacity, rz_producer** out) {
+    if (!ctx || !out || capacity < 1 || cand_capacity < 0) return RZ_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (capacity > int64_t(kProducedMaxK) || cand_capacity > int64_t(1) << 24) return RZ_ERR_UNSUPPORTED;
+    if (produced_smem_bytes(uint32_t(capacity)) + 4096 > ctx->smem_optin) return RZ_ERR_UNSUPPORTED;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    rz_producer* p = new (std::nothrow) rz_producer();
+    if (!p) return RZ_ERR_NO_MEMORY;
+    p->ctx = ctx;
+    p->capacity = uint32_t(capacity);
+    p->cand_capacity = uint32_t(cand_capacity);
+    // One allocation: counts (256 bytes) | list | candidates.
+    const size_t list_bytes = (size_t(capacity) * 4 + 255) / 256 * 256;
+    const size_t bytes = 256 + list_bytes + size_t(std::max<int64_t>(cand_capacity, 1)) * 8;
+    void* mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, bytes);
+    if (e == cudaSuccess) e = cudaMemset(mem, 0, 256);
+    if (e != cudaSuccess) {
+        if (mem) cudaFree(mem);
+        delete p;
+        return e == cudaErrorMemoryAllocation ? RZ_ERR_NO_MEMORY : cuda_fail(ctx, e, "producer buffers");
+    }
+    uint8_t* b = static_cast<uint8_t*>(mem);
+    p->counts = reinterpret_cast<uint32_t*>(b);
+    p->idx = reinterpret_cast<uint32_t*>(b + 256);
+    p->cand = reinterpret_cast<uint32_t*>(b + 256 + list_bytes);
+    *out = p;
+    return RZ_OK;
+}
+
+void rz_producer_destroy(rz_producer* p) {
+    if (!p) return;
+    cudaSetDevice(p->ctx->device);
+    cudaDeviceSynchronize();
+    cudaFree(p->counts);
+    delete p;
+}
+
+int rz_producer_reset(rz_producer* p, int64_t n, rz_stream_t stream) {
+    if (!p || n < 1) return RZ_ERR_INVALID_ARG;
+    if (n >= (int64_t(1) << 32)) return RZ_ERR_UNSUPPORTED;
+    std::lock_guard<std::recursive_mutex> g(p->ctx->mu);
+    cudaSetDevice(p->ctx->device);
+    RZ_CUDA_TRY(p->ctx, cudaMemsetAsync(p->counts, 0, 2 * sizeof(uint32_t), reinterpret_cast<cudaStream_t>(stream)));
+    p->n = uint32_t(n);
+    p->have_n = true;
+    return RZ_OK;
+}
+
+int rz_producer_get_view(const rz_producer* p, rz_producer_view* out) {
+    if (!p || !out || !p->have_n) return RZ_ERR_INVALID_ARG;
+    out->idx = p->idx;
+    out->counts = p->counts;
+    out->cand = p->cand;
+    out->capacity = p->capacity;
+    out->cand_capacity = p->cand_capacity;
+    out->n = p->n;
+    out->floor = p->n > p->capacity ? p->n - p->capacity : 0u;
+    return RZ_OK;
+}
+
+int rz_produce_where_less(rz_producer* p, const uint32_t* d_keys, uint32_t threshold, rz_stream_t stream) {
+    if (!p || !d_keys || !p->have_n) return RZ_ERR_INVALID_ARG;
+    rz_ctx* ctx = p->ctx;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    rz_producer_view v;
+    rz_producer_get_view(p, &v);
+    const int grid = std::max(1, std::min<int>(ctx->sms * 8, int((uint64_t(p->n) + 255) / 256)));
+    produce_where_less_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(v, d_keys, threshold);
+    RZ_CUDA_TRY(ctx, cudaGetLastError());
+    return RZ_OK;
+}
+
+int rz_producer_download(const rz_producer* p, uint32_t* h_idx, int64_t max, int64_t* k, int64_t* candidates,
+                         rz_stream_t stream) {
+    if (!p || max < 0 || (max > 0 && !h_idx)) return RZ_ERR_INVALID_ARG;
+    rz_ctx* ctx = p->ctx;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t c[2] = {0, 0};
+    RZ_CUDA_TRY(ctx, cudaMemcpyAsync(c, p->counts, sizeof(c), cudaMemcpyDeviceToHost, s));
+    RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    const int64_t m = std::min<int64_t>(std::min<int64_t>(c[0], p->capacity), max);
+    if (m > 0) {
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(h_idx, p->idx, size_t(m) * 4, cudaMemcpyDeviceToHost, s));
+        RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    }
+    if (k) *k = c[0];
+    if (candidates) *candidates = c[1];
+    return RZ_OK;
+}
+
+int rz_remove_produced(rz_ctx* ctx, rz_producer* p, void* d_data, uint32_t elem_bytes, int64_t* new_len,
+                       uint32_t flags, rz_stream_t stream) {
+    if (!ctx || !p || !d_data || !p->have_n) return RZ_ERR_INVALID_ARG;
+    if (elem_bytes != 4 && elem_bytes != 8 && elem_bytes != 16 && elem_bytes != 32) return RZ_ERR_INVALID_ARG;
+    if (reinterpret_cast<uintptr_t>(d_data) % (elem_bytes >= 16 ? 16 : elem_bytes)) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int st = reset_if_dirty(ctx, s);
+    if (st != RZ_OK) return st;
+    ctx->last_kernels = 0;
+    const bool validate = (flags & RZ_VALIDATE) != 0;
+    if (validate) {
+        // The validation passes need k on the host: the one synchronisation of this path.
+        uint32_t hk = 0;
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(&hk, p->counts, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        RZ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+        if (hk > p->capacity) {
+            if (new_len) *new_len = int64_t(p->n) - int64_t(hk);
+            return RZ_ERR_NO_MEMORY;
+        }
+        if (hk > 0) {
+            st = launch_validate(ctx, p->n, p->idx, hk, s);
+            if (st != RZ_OK) return st;
+            ctx->last_kernels += 2;
+        }
+    }
+    // About 64 tiles for a full list: 256 threads, 1..8 items each.
+    int items = 1;
+    while (items < 8 && uint64_t(kProducedBlock) * items * 64 < p->capacity) items *= 2;
+    ProducedFn f = produced_fn(elem_bytes, items);
+    if (!f) return RZ_ERR_INVALID_ARG;
+    const size_t smem = produced_smem_bytes(p->capacity);
+    static std::atomic<uint64_t> attr_done[4][4];
+    const int wi = elem_bytes == 4 ? 0 : elem_bytes == 8 ? 1 : elem_bytes == 16 ? 2 : 3;
+    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    if (!(attr_done[wi][ii].load() & bit)) {
+        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              int(ctx->smem_optin) - 4096));
+        attr_done[wi][ii].fetch_or(bit);
+    }
+    const uint32_t tile = uint32_t(kProducedBlock) * uint32_t(items);
+    const uint32_t grid = std::max<uint32_t>(1u, (p->capacity + tile - 1) / tile);
+    ProducedParams pp;
+    pp.data = static_cast<uint8_t*>(d_data);
+    pp.idx = p->idx;
+    pp.counts = p->counts;
+    pp.cand = reinterpret_cast<const uint2*>(p->cand);
+    pp.n = p->n;
+    pp.capacity = p->capacity;
+    pp.cand_capacity = p->cand_capacity;
+    pp.status = ctx->ws.status;
+    pp.dev_len = ctx->ws.dev_len;
+    pp.validate = validate ? 1u : 0u;
+    f<<<grid, kProducedBlock, smem, s>>>(pp);
+    RZ_CUDA_TRY(ctx, cudaGetLastError());
+    ctx->last_kernels += 1;
+    ctx->last_grid = int(grid);
+    ctx->last_block = kProducedBlock;
+    if (flags & RZ_SYNC) return read_status(ctx, s, new_len);
+    if (new_len) *new_len = -1;  // on the device until the stream reaches this point
+    return RZ_OK;
+}
+
+}  // extern "C"

@@ -55,3 +55,26 @@ def test_workload_distributions():
     assert (r >= n - 1000).sum() == 250
     nn, kk = workloads.batched_lists(4096, seed=0)
     assert nn.min() >= 256 and nn.max() <= 1 << 22 and (kk <= nn // 2 + 1).all()
+
+
+def test_device_producer_header_compiles_in_a_caller_kernel(tmp_path):
+    """include/redzone_device.cuh is usable from a caller's own CUDA file (compiled for sm_100a
+    here; running it is the GPU tests' job)."""
+    import os
+    import pytest
+    nvcc = "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.cu"
+    src.write_text(
+        '#include "redzone_device.cuh"\n'
+        "__global__ void delete_small(rz_producer_view v, const float* score, uint32_t n) {\n"
+        "    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ((n + 31u) & ~31u);\n"
+        "         i += gridDim.x * blockDim.x)\n"
+        "        rz_emit(v, i, i < n && score[i] < 0.5f);\n"
+        "}\n")
+    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-c", str(src), "-o",
+                        str(tmp_path / "caller.o"), "-I", os.path.join(root, "include")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
