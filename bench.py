@@ -15,6 +15,9 @@ partition comparator on the same workload, an end-to-end figure through rz_remov
 (removal list copied from pinned host memory, new length read back, every step), the
 reference's own CPU Redzone timed on this host, and SM clocks sampled during the timed region.
 
+Other workloads: --workload batched (4096 lists, one launch), --workload service (streaming
+deletes), --workload produced (a list made on the GPU with fused red-zone marking), --sweep (k).
+
 Reference arm (--impl reference): the reference's redzone_CPU (compiled from its sources into
 oracle/_ref) on the same workload on the host cores, rank 0 only.
 """
@@ -601,6 +604,101 @@ def ctypes_byref(x):
     return ctypes.byref(x)
 
 
+def produced(args):
+    """Removal of a list made on the GPU with fused red-zone marking (rz_emit / rz_remove_produced)
+    against rz_remove on the same list: n = 2^28 int32 rows, a producer that deletes every row
+    whose uint32 key is below a threshold (k = 2^16 of them, uniform), L2 flushed between steps."""
+    import torch
+    import redzone_b200 as rz
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    ctx = rz.Context(0)
+    n, k = 1 << N_LOG2, 1 << K_LOG2
+    scrub = torch.empty(SCRUB_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    a = torch.arange(n, dtype=torch.int32, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(args.seed)
+    keys = torch.randint(1 << 30, (1 << 31) - 1, (n,), device=dev, dtype=torch.int32, generator=g)
+    keys[torch.randperm(n, device=dev, generator=g)[:k]] = 5
+    thr = 1 << 30
+    prod = rz.Producer(ctx, capacity=k, cand_capacity=4096)
+    prod.reset(n)
+    prod.produce_where_less(keys, thr)
+    lst, kk, cands = prod.download()
+    assert kk == k
+    d_list = torch.from_numpy(lst.view(np.int32)).to(dev)
+    # Parity gate: both paths give the same bits on the same list.
+    a2 = a.clone()
+    prod.remove(a, flags=rz.RZ_SYNC)
+    ctx.remove(a2, d_list, flags=rz.RZ_SYNC)
+    assert torch.equal(a, a2), "produced and index-list removals differ"
+    del a2
+
+    def ev_mean(fn, steps):
+        for i in range(args.warmup):
+            fn()
+            scrub.fill_(i & 255)
+        ev = []
+        for i in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            scrub.fill_(i & 255)
+            ev.append((e0, e1))
+        torch.cuda.synchronize()
+        return statistics.mean(s.elapsed_time(e) for s, e in ev)
+
+    def steady(fn):
+        ms = []
+        for with_fn in (True, False):
+            gr = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gr):
+                for i in range(NSETS):
+                    if with_fn:
+                        fn()
+                    scrub.fill_(i & 255)
+            gr.replay()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(100):
+                gr.replay()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            del gr
+        return (ms[0] - ms[1]) / (100 * NSETS)
+
+    steps = min(args.steps, 1000)
+    t_prod = ev_mean(lambda: prod.remove(a), steps)
+    t_list = ev_mean(lambda: ctx.remove(a, d_list), steps)
+    s_prod, s_list = steady(lambda: prod.remove(a)), steady(lambda: ctx.remove(a, d_list))
+
+    def round_fused():
+        prod.reset(n)
+        prod.produce_where_less(keys, thr)
+        prod.remove(a)
+
+    t_round = ev_mean(round_fused, min(steps, 200))
+    print(json.dumps({
+        "metric": METRIC, "value": k / (t_prod * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t_prod, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "removal of a GPU-produced list with fused red-zone marking, n=2^28 int32, "
+                               "k=2^16 rows whose uint32 key is below a threshold (uniform)",
+                   "n": n, "k": k, "elem_bytes": 4, "capacity": k, "candidates": cands,
+                   "l2": "flushed between timed steps (256 MiB scrub write)", "parallelism": "single GPU"},
+        "index_list_same_rows": {"ms_per_step": t_list, "items_per_s": k / (t_list * 1e-3)},
+        "graph_steady_state": {"produced_ms": s_prod, "index_list_ms": s_list},
+        "producer_and_removal_round_ms": t_round,
+        "gpu_launches": steps,
+    }), flush=True)
+    prod.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -610,7 +708,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--sweep", action="store_true", help="run the k sweep instead of the headline")
     ap.add_argument("--sweep-k", default="", help="comma-separated log2(k) values for --sweep")
-    ap.add_argument("--workload", choices=["single", "batched", "service"], default="single")
+    ap.add_argument("--workload", choices=["single", "batched", "service", "produced"], default="single")
     ap.add_argument("--shards", type=int, default=16, help="--workload service: table shards")
     ap.add_argument("--slots", type=int, default=4, help="--workload service: concurrent launch slots")
     ap.add_argument("--max-batches", type=int, default=16, help="--workload service: batches per launch")
@@ -643,6 +741,8 @@ def main():
         batched(args)
     elif args.workload == "service":
         service(args)
+    elif args.workload == "produced":
+        produced(args)
     else:
         own_arm(args)
 

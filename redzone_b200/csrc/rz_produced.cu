@@ -217,13 +217,35 @@ static ProducedFn produced_fn(uint32_t w, int items) {
     }
 }
 
-// The library's own producer: every row i < n with keys[i] < threshold.
+// The library's own producer: every row i < n with keys[i] < threshold. Each thread reads 16
+// keys per step (four 16-byte loads in flight: a 4-byte load per step would leave the kernel
+// waiting on memory latency) and emits them warp-wide; keys not 16-byte aligned, and the last
+// n % 16, take the one-key loop.
 __global__ void produce_where_less_kernel(const rz_producer_view v, const uint32_t* __restrict__ keys,
-                                          uint32_t threshold) {
+                                          uint32_t threshold, uint32_t vec) {
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t gtid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint64_t nvec = vec ? v.n / 16u : 0u;
     // Every lane of a warp runs the same number of iterations (rz_emit is called warp-wide).
-    const uint64_t n_round = (uint64_t(v.n) + 31u) & ~uint64_t(31);
-    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+    const uint64_t nvec_round = (nvec + 31u) & ~uint64_t(31);
+    for (uint64_t c = gtid; c < nvec_round; c += stride) {
+        const bool ok = c < nvec;
+        uint4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            q[u] = ok ? __ldg(reinterpret_cast<const uint4*>(keys) + c * 4 + u) : make_uint4(~0u, ~0u, ~0u, ~0u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t row = uint32_t(c * 16 + 4 * u);
+            rz_emit(v, row, ok && q[u].x < threshold);
+            rz_emit(v, row + 1, ok && q[u].y < threshold);
+            rz_emit(v, row + 2, ok && q[u].z < threshold);
+            rz_emit(v, row + 3, ok && q[u].w < threshold);
+        }
+    }
+    const uint64_t rest = nvec * 16;
+    const uint64_t n_round = rest + ((uint64_t(v.n) - rest + 31u) & ~uint64_t(31));
+    for (uint64_t i = rest + gtid; i < n_round; i += stride) {
         const bool take = i < v.n && __ldg(&keys[i]) < threshold;
         rz_emit(v, uint32_t(i), take);
     }
@@ -304,8 +326,10 @@ int rz_produce_where_less(rz_producer* p, const uint32_t* d_keys, uint32_t thres
     cudaSetDevice(ctx->device);
     rz_producer_view v;
     rz_producer_get_view(p, &v);
-    const int grid = std::max(1, std::min<int>(ctx->sms * 8, int((uint64_t(p->n) + 255) / 256)));
-    produce_where_less_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(v, d_keys, threshold);
+    const uint32_t vec = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0 ? 1u : 0u;
+    const uint64_t units = vec ? (uint64_t(p->n) + 15) / 16 : uint64_t(p->n);
+    const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->sms) * 8, (units + 255) / 256)));
+    produce_where_less_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(v, d_keys, threshold, vec);
     RZ_CUDA_TRY(ctx, cudaGetLastError());
     return RZ_OK;
 }

@@ -145,3 +145,16 @@ def test_capacity_exceeded_moves_nothing(ctx):
     # The context is usable afterwards.
     run_round(ctx, prod, host, keys_for(n, 3000, seed=9))
     prod.close()
+
+
+def test_producer_with_unaligned_keys(ctx):
+    """Keys that do not start on a 16-byte boundary take the one-key loop: same rows emitted."""
+    n, k = 100003, 3000
+    keys = keys_for(n, k, seed=31)
+    buf = torch.from_numpy(np.concatenate([[0], keys]).astype(np.uint32).view(np.int32)).to(DEV)
+    prod = rz.Producer(ctx, capacity=4096)
+    prod.reset(n)
+    prod.produce_where_less(buf[1:], 1 << 31)
+    lst, kk, _ = prod.download()
+    assert kk == k and sorted(lst.tolist()) == sorted(np.flatnonzero(keys < (1 << 31)).tolist())
+    prod.close()
