@@ -66,6 +66,8 @@ typedef enum rz_status {
 #define RZ_SCHED_CLUSTER 2  /* one thread-block cluster; red-zone bitmap in distributed smem      */
 #define RZ_SCHED_GRID    3  /* persistent grid, bounded global barriers                           */
 #define RZ_SCHED_CSCAN   4  /* independent 8-CTA clusters, each finds every red entry; no grid wait */
+#define RZ_SCHED_SPLIT   5  /* a scan grid lists the red entries; the pairing grid (launched as its */
+                            /* programmatic dependent) reads them; no wait inside either grid     */
 
 /* Launch configuration of the single-list kernels (one entry of the 56-point tuning space:
  * block x items x grid scale with the schedule chosen by k, or a cluster-scan launch; plus the

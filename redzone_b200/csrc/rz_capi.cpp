@@ -85,6 +85,7 @@ int reset_if_dirty(rz_ctx* ctx, cudaStream_t s) {
     if (w.seen) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.seen, 0, w.seen_words * 4, s));
     if (w.part_bits) RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.part_bits, 0, w.part_words * 4, s));
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.epoch, 0, 4, s));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.split_count, 0, 8, s));
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.arrive, 0, kMaxGrid * 4, s));
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.cnt_words, 0, 2 * kMaxGrid * 8, s));
     RZ_CUDA_TRY(ctx, cudaMemsetAsync(w.arrive64, 0, kMaxGrid * 8, s));
@@ -190,7 +191,8 @@ int rz_create(rz_ctx** out, int device) {
     ctx->smem_optin = prop.sharedMemPerBlockOptin;
     Workspace& w = ctx->ws;
     void* p = nullptr;
-    // One allocation: status | epoch | dev_len (one 256-byte line each) | arrival tags |
+    // One allocation: status | epoch (split-schedule counters at +128) | dev_len (one 256-byte
+    // line each) | arrival tags |
     // tagged orphan counts | tagged red-entry counts | phase stamps.
     const size_t off_arrive = 768;
     const size_t off_cnt = off_arrive + size_t(kMaxGrid) * 4;
@@ -207,6 +209,7 @@ int rz_create(rz_ctx** out, int device) {
     uint8_t* b = static_cast<uint8_t*>(p);
     w.status = reinterpret_cast<uint32_t*>(b);
     w.epoch = reinterpret_cast<uint32_t*>(b + 256);
+    w.split_count = reinterpret_cast<uint32_t*>(b + 384);
     w.dev_len = reinterpret_cast<unsigned long long*>(b + 512);
     w.arrive = reinterpret_cast<uint32_t*>(b + off_arrive);
     w.cnt_words = reinterpret_cast<unsigned long long*>(b + off_cnt);

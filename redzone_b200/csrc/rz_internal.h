@@ -43,6 +43,7 @@ struct Workspace {
     uint4* keep_stage = nullptr;     // rz_keep: the kept items, 16-byte units
     size_t keep_cap = 0;
     uint32_t* epoch = nullptr;       // grid schedule: call epoch (advanced by CTA 0 each call)
+    uint32_t* split_count = nullptr; // split schedule: red entries listed, pairing CTAs done (reset by the last)
     uint32_t* arrive = nullptr;      // grid schedule: per-CTA arrival tags, kMaxGrid
     unsigned long long* cnt_words = nullptr;  // grid schedule: tagged orphan counts, 2*kMaxGrid
     unsigned long long* arrive64 = nullptr;   // red-list schedule: tag << 32 | red entries, kMaxGrid
@@ -112,6 +113,9 @@ constexpr uint32_t kCscanMinK = (1u << 12) + 1;  // the default uses the cluster
 constexpr uint32_t kCscanMaxK = 1u << 17;       // ... to here (one register pass per slice)
 // Cluster schedule (rz_cluster.cu); RZ_ERR_UNSUPPORTED when the bitmap slice does not fit in
 // shared memory or no cluster of the requested size can be co-scheduled.
+// Split schedule (rz_produced.cu); RZ_ERR_UNSUPPORTED for k > kFastMaxK or too little shared memory.
+int launch_split(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
+                 const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                    const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int cluster_max_block(int w, int items);

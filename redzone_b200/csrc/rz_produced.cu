@@ -45,21 +45,27 @@ static size_t produced_smem_bytes(uint32_t capacity) {
     return (pairfill_words((capacity + 31) / 32) + 2 * size_t(kFastMaxRed)) * 4;
 }
 
+// Produced lists: k = counts[0], candidates counted in counts[1]. Split schedule (rz_remove with
+// a device index list, see below): k = k_fixed, candidates counted in *cand_count, written by the
+// scan kernel this kernel waits for (pdl); the last CTA to read the count resets it (done).
 struct ProducedParams {
     uint8_t* data;
     const uint32_t* idx;
-    const uint32_t* counts;
+    const uint32_t* counts;      // produced lists only
+    const uint32_t* cand_count;  // counts + 1, or the split scan's counter
+    uint32_t* done;              // split schedule: CTAs that have read *cand_count
     const uint2* cand;
-    uint32_t n, capacity, cand_capacity;
+    uint32_t n, k_fixed, capacity, cand_capacity;
     uint32_t* status;
     unsigned long long* dev_len;
     uint32_t validate;
+    uint32_t pdl;                // wait for the preceding (scan) grid before reading candidates
 };
 
 template <int W, int IPT>
 __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(const ProducedParams p) {
     using T = typename Payload<W>::T;
-    const uint32_t k = __ldcg(&p.counts[0]), m = __ldcg(&p.counts[1]);
+    const uint32_t k = p.k_fixed ? p.k_fixed : __ldcg(&p.counts[0]);
     const uint32_t n = p.n;
     if (k > p.capacity) {  // uniform: every CTA reads the same counts
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.status, ST_CAPACITY);
@@ -87,7 +93,7 @@ __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(con
     uint32_t* s_val = pf.val();
     uint32_t* u_pos = s_dyn + pairfill_words(kwc);  // red entries as collected (any order)
     uint32_t* u_val = u_pos + kFastMaxRed;
-    __shared__ uint32_t s_R;
+    __shared__ uint32_t s_R, s_m;
     __shared__ int s_abort;
 
     if (threadIdx.x == 0) {
@@ -109,8 +115,22 @@ __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(con
         mapV[w] = 0u;
         mapP[w] = 0u;
     }
+    // Everything above overlaps the scan grid of the split schedule; the candidates need it done.
+    if (p.pdl) asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (threadIdx.x == 0) {
+        s_m = __ldcg(p.cand_count);
+        if (p.done) {
+            // Self-cleaning counter: the last CTA to have read it resets it for the next call.
+            __threadfence();
+            if (atomicAdd(p.done, 1u) == gridDim.x - 1) {
+                *const_cast<uint32_t*>(p.cand_count) = 0u;
+                *p.done = 0u;
+            }
+        }
+    }
     __syncthreads();
     if (s_abort) return;  // validation failed: nothing moves
+    const uint32_t m = s_m;
 
     // ---- the red entries: from the candidates, or (candidates overflowed) from the whole list ---
     const bool from_cand = m <= p.cand_capacity;
@@ -217,6 +237,55 @@ static ProducedFn produced_fn(uint32_t w, int items) {
     }
 }
 
+// Split schedule, first grid: every red entry (i, idx[i] >= cut) of a device index list, appended
+// (any order) to a candidate buffer with one atomic per warp; out-of-range entries are reported.
+// The pairing grid is launched as its programmatic dependent, so its tile loads overlap this.
+__global__ void __launch_bounds__(256) split_scan_kernel(const uint32_t* __restrict__ idx, uint32_t k, uint32_t n,
+                                                         uint32_t vec, uint2* __restrict__ cand,
+                                                         uint32_t* __restrict__ cand_count, uint32_t* status) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const uint32_t cut = n - k;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const uint32_t nq = vec ? k / 4 : 0;
+    const uint32_t lane = threadIdx.x & 31;
+    // Every lane of a warp runs the same number of iterations (the append is warp-wide).
+    const uint32_t total = nq + (k - 4 * nq);  // quads, then the remaining single entries
+    const uint32_t total_round = (total + 31u) & ~31u;
+    bool oor = false;
+    for (uint32_t u = gtid; u < total_round; u += stride) {
+        uint32_t e0, v[4], cnt = 0;
+        if (u < nq) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(idx) + u);
+            e0 = 4 * u;
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+            cnt = 4;
+        } else {
+            e0 = 4 * nq + (u - nq);
+            v[0] = u < total ? __ldg(&idx[e0]) : 0u;
+            v[1] = v[2] = v[3] = 0u;
+            cnt = u < total ? 1u : 0u;
+        }
+        uint32_t redbits = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const bool in = uint32_t(c) < cnt;
+            oor |= in && v[c] >= n;
+            redbits |= uint32_t(in && v[c] >= cut && v[c] < n) << c;
+        }
+        const uint32_t mine = uint32_t(__popc(redbits));
+        const uint32_t inc = warp_inclusive_scan(mine);
+        const uint32_t wtot = __shfl_sync(0xffffffffu, inc, 31);
+        if (wtot == 0u) continue;
+        uint32_t base = 0;
+        if (lane == 31) base = atomicAdd(cand_count, wtot);
+        base = __shfl_sync(0xffffffffu, base, 31) + inc - mine;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if ((redbits >> c) & 1u) cand[base++] = make_uint2(e0 + uint32_t(c), v[c]);
+    }
+    if (__any_sync(0xffffffffu, oor) && lane == 0) atomicOr(status, ST_RANGE);
+}
+
 // The library's own producer: every row i < n with keys[i] < threshold. Each thread reads 16
 // keys per step (four 16-byte loads in flight: a 4-byte load per step would leave the kernel
 // waiting on memory latency) and emits them warp-wide; keys not 16-byte aligned, and the last
@@ -249,6 +318,71 @@ __global__ void produce_where_less_kernel(const rz_producer_view v, const uint32
         const bool take = i < v.n && __ldg(&keys[i]) < threshold;
         rz_emit(v, uint32_t(i), take);
     }
+}
+
+// Split schedule of rz_remove (RZ_SCHED_SPLIT): the scan grid above, then the pairing grid of the
+// produced-list path as its programmatic dependent. One 256 * items tile per pairing CTA;
+// RZ_ERR_UNSUPPORTED when the shared-memory maps would not fit or k > kFastMaxK.
+int launch_split(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
+                 const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info) {
+    if (k == 0 || k > kFastMaxK || !ctx->ws.redlist || ctx->ws.red_cap < size_t(k) + 1) return RZ_ERR_UNSUPPORTED;
+    const size_t smem = produced_smem_bytes(k);
+    if (smem + 4096 > ctx->smem_optin) return RZ_ERR_UNSUPPORTED;
+    int items = cfg.items;
+    ProducedFn f = produced_fn(w, items);
+    if (!f) return RZ_ERR_INVALID_ARG;
+    static std::atomic<uint64_t> attr_done[4][4];
+    const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
+    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    if (!(attr_done[wi][ii].load() & bit)) {
+        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              int(ctx->smem_optin) - 4096));
+        attr_done[wi][ii].fetch_or(bit);
+    }
+    const uint32_t vec = (reinterpret_cast<uintptr_t>(idx) & 15u) == 0 ? 1u : 0u;
+    const uint32_t units = vec ? k / 4 + (k & 3u) : k;
+    const uint32_t sgrid = std::max<uint32_t>(1u, std::min<uint32_t>((units + 255) / 256, uint32_t(ctx->sms) * 4));
+    uint2* cand = ctx->ws.redlist;
+    uint32_t* counter = ctx->ws.split_count;
+    split_scan_kernel<<<sgrid, 256, 0, s>>>(idx, k, n, vec, cand, counter, ctx->ws.status);
+    RZ_CUDA_TRY(ctx, cudaGetLastError());
+
+    const uint32_t tile = uint32_t(kProducedBlock) * uint32_t(items);
+    const uint32_t grid = (k + tile - 1) / tile;
+    ProducedParams pp;
+    pp.data = static_cast<uint8_t*>(data);
+    pp.idx = idx;
+    pp.counts = nullptr;
+    pp.cand_count = counter;
+    pp.done = counter + 1;
+    pp.cand = cand;
+    pp.n = n;
+    pp.k_fixed = k;
+    pp.capacity = k;
+    pp.cand_capacity = k + 1;
+    pp.status = ctx->ws.status;
+    pp.dev_len = ctx->ws.dev_len;
+    pp.validate = validate ? 1u : 0u;
+    pp.pdl = 1;
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(kProducedBlock);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    RZ_CUDA_TRY(ctx, cudaLaunchKernelEx(&lc, f, pp));
+    if (info) {
+        info->grid = int(grid);
+        info->block = kProducedBlock;
+        info->items = items;
+        info->launches += 2;
+    }
+    return RZ_OK;
 }
 
 }  // namespace rz
@@ -402,13 +536,17 @@ int rz_remove_produced(rz_ctx* ctx, rz_producer* p, void* d_data, uint32_t elem_
     pp.data = static_cast<uint8_t*>(d_data);
     pp.idx = p->idx;
     pp.counts = p->counts;
+    pp.cand_count = p->counts + 1;
+    pp.done = nullptr;
     pp.cand = reinterpret_cast<const uint2*>(p->cand);
     pp.n = p->n;
+    pp.k_fixed = 0;
     pp.capacity = p->capacity;
     pp.cand_capacity = p->cand_capacity;
     pp.status = ctx->ws.status;
     pp.dev_len = ctx->ws.dev_len;
     pp.validate = validate ? 1u : 0u;
+    pp.pdl = 0;
     f<<<grid, kProducedBlock, smem, s>>>(pp);
     RZ_CUDA_TRY(ctx, cudaGetLastError());
     ctx->last_kernels += 1;

@@ -206,6 +206,17 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     if (flags & RZ_FORCE_BLOCK) sched = RZ_SCHED_BLOCK;
     if (flags & RZ_FORCE_GRID) sched = RZ_SCHED_GRID;
     if (sched == RZ_SCHED_AUTO) sched = (k <= kClusterMaxK) ? RZ_SCHED_CLUSTER : RZ_SCHED_GRID;
+    if (sched == RZ_SCHED_SPLIT) {
+        LaunchInfo ci;
+        ci.launches = launches;
+        st = launch_split(ctx, data, n, w, idx, k, cfg, validate, s, &ci);
+        if (st == RZ_OK) {
+            if (info) *info = ci;
+            return RZ_OK;
+        }
+        if (st != RZ_ERR_UNSUPPORTED) return st;
+        sched = RZ_SCHED_GRID;  // k beyond the shared-memory maps
+    }
     if (sched == RZ_SCHED_CSCAN) {
         LaunchInfo ci;
         ci.launches = launches;

@@ -71,10 +71,10 @@ def test_widths_and_distributions(ctx, words, dist):
         assert np.array_equal(got[n - k:], host[n - k:]), "tail must be left untouched"
 
 
-SCHEDULES = {"cluster": 2, "grid": 3, "cscan": 4}
+SCHEDULES = {"cluster": 2, "grid": 3, "cscan": 4, "split": 5}
 
 
-@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan"])
+@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan", "split"])
 def test_every_launch_config_gives_the_same_bits(ctx, sched):
     """The result depends only on (data, idx), never on schedule, block, items or grid."""
     cases = [(1 << 20, 1 << 16, "uniform"), (1 << 18, 1 << 17, "red50"), (1 << 16, 3001, "red100")]
@@ -91,7 +91,7 @@ def test_every_launch_config_gives_the_same_bits(ctx, sched):
                         assert np.array_equal(got[: n - k], exp[: n - k]), (sched, n, k, dist, words, block, items, cps)
 
 
-@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan"])
+@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan", "split"])
 @pytest.mark.parametrize("words", [1, 2, 4, 8])
 def test_schedules_on_large_k(ctx, sched, words):
     n = 1 << 21
@@ -151,7 +151,8 @@ def test_n64_every_k_multi_cta(ctx, words):
             idx = rng.permutation(n)[:k].astype(np.uint32)
             exp = expect_of(host, idx)
             for cfg, fl in ((rz.LaunchCfg(32, 1, 4, 0, 3), rz.RZ_FORCE_GRID), (rz.LaunchCfg(32, 2, 4, 0, 3), rz.RZ_FORCE_GRID),
-                            (rz.LaunchCfg(32, 1, 4, 0, 4), 0), (rz.LaunchCfg(32, 4, 1, 0, 4), 0)):
+                            (rz.LaunchCfg(32, 1, 4, 0, 4), 0), (rz.LaunchCfg(32, 4, 1, 0, 4), 0),
+                            (rz.LaunchCfg(32, 1, 1, 0, 5), 0)):
                 got = run_gpu(ctx, host, idx, cfg=cfg, flags=fl | rz.RZ_SYNC)
                 assert np.array_equal(got[: n - k], exp[: n - k]), (words, k, rep, cfg)
 
@@ -166,6 +167,41 @@ def test_back_to_back_calls_leave_scratch_clean(ctx):
         idx = workloads.uniform(n, k, seed=it)
         got = run_gpu(ctx, host, idx)
         assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k]), it
+
+
+def test_split_schedule_back_to_back_and_under_graph_replay(ctx):
+    """The split schedule's scan counter is reset by its own pairing grid: calls in a row, and one
+    call captured in a CUDA graph replayed several times, stay exact."""
+    cfg = rz.LaunchCfg(256, 4, 1, 0, 5)
+    rng = np.random.default_rng(3)
+    for it in range(10):
+        n = int(rng.integers(1 << 12, 1 << 20))
+        k = int(rng.integers(1, min(n, 1 << 17)))
+        host = payload(n, 1, seed=it)
+        idx = workloads.make("red50" if it % 3 == 0 else "uniform", n, k, seed=it)
+        got = run_gpu(ctx, host, idx, cfg=cfg)
+        assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k]), it
+    n, k = 1 << 20, 1 << 15
+    host = payload(n, 1, seed=40)
+    idx = workloads.uniform(n, k, seed=40)
+    exp = expect_of(host, idx)
+    d0 = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    d = d0.clone()
+    di = torch.from_numpy(idx.astype(np.int32)).to(DEV)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        ctx.remove_cfg(d, di, cfg, stream=s)  # first call outside the capture
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            ctx.remove_cfg(d, di, cfg, stream=s)
+    for rep in range(3):
+        d.copy_(d0)
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(d.cpu().numpy().view(np.uint32).reshape(n, 1)[: n - k], exp[: n - k]), rep
+    del g
 
 
 def test_validation_reports_and_leaves_data_untouched(ctx):
@@ -190,13 +226,15 @@ def test_validation_reports_and_leaves_data_untouched(ctx):
     assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
 
 
-def test_validation_on_the_cluster_scan_schedule(ctx):
-    """A failed validation on the cluster-scan schedule leaves the data untouched (its CTAs still
-    meet at every cluster barrier phase), and the next call is exact."""
+@pytest.mark.parametrize("sched", [4, 5])
+def test_validation_on_the_cluster_scan_and_split_schedules(ctx, sched):
+    """A failed validation on the cluster-scan schedule (whose CTAs still meet at every cluster
+    barrier phase) or the split schedule (whose pairing CTAs still reset the scan's counter)
+    leaves the data untouched, and the next call is exact."""
     n, k = 1 << 18, 1 << 14
     host = payload(n, 2, seed=9)
     idx = workloads.uniform(n, k, seed=9)
-    cfg = rz.LaunchCfg(256, 4, 1, 0, 4)
+    cfg = rz.LaunchCfg(256, 4, 1, 0, sched)
     for bad_at, bad_val, code in ((100, None, 2), (7, n + 3, 3)):
         bad = idx.copy()
         bad[bad_at] = bad[bad_at + 1] if bad_val is None else bad_val
@@ -265,7 +303,8 @@ def test_red_list_schedule_around_its_limit(ctx, red, words):
     host = payload(n, words, seed=red)
     exp = expect_of(host, idx)
     for cfg in (None, rz.LaunchCfg(256, 4, 1, 0, 3), rz.LaunchCfg(128, 2, 4, 0, 3), rz.LaunchCfg(256, 4, 1, 0, 4),
-                rz.LaunchCfg(128, 2, 4, 0, 4), rz.LaunchCfg(64, 1, 4, 0, 4)):
+                rz.LaunchCfg(128, 2, 4, 0, 4), rz.LaunchCfg(64, 1, 4, 0, 4), rz.LaunchCfg(256, 4, 1, 0, 5),
+                rz.LaunchCfg(256, 1, 1, 0, 5)):
         got = run_gpu(ctx, host, idx, cfg=cfg)
         assert np.array_equal(got[: n - k], exp[: n - k]), (red, words, cfg)
 
