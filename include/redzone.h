@@ -68,6 +68,7 @@ typedef enum rz_status {
 #define RZ_SCHED_CSCAN   4  /* independent 8-CTA clusters, each finds every red entry; no grid wait */
 #define RZ_SCHED_SPLIT   5  /* a scan grid lists the red entries; the pairing grid (launched as its */
                             /* programmatic dependent) reads them; no wait inside either grid     */
+#define RZ_SCHED_SCANALL 6  /* one grid, every CTA reads the whole list; no wait (short lists)    */
 
 /* Launch configuration of the single-list kernels (one entry of the 56-point tuning space:
  * block x items x grid scale with the schedule chosen by k, or a cluster-scan launch; plus the

@@ -23,7 +23,7 @@ c_vp, c_i32, c_u32, c_i64, c_u64, c_f32 = (ctypes.c_void_p, ctypes.c_int32, ctyp
                                            ctypes.c_int64, ctypes.c_uint64, ctypes.c_float)
 
 
-RZ_SCHED_AUTO, RZ_SCHED_BLOCK, RZ_SCHED_CLUSTER, RZ_SCHED_GRID, RZ_SCHED_CSCAN, RZ_SCHED_SPLIT = 0, 1, 2, 3, 4, 5
+RZ_SCHED_AUTO, RZ_SCHED_BLOCK, RZ_SCHED_CLUSTER, RZ_SCHED_GRID, RZ_SCHED_CSCAN, RZ_SCHED_SPLIT, RZ_SCHED_SCANALL = 0, 1, 2, 3, 4, 5, 6
 
 
 class LaunchCfg(ctypes.Structure):

@@ -109,6 +109,7 @@ int launch_cscan(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t
                  const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 // The default cluster-scan launch for (k, w), if that schedule runs it: false otherwise.
 bool cscan_default_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
+constexpr uint32_t kScanAllMaxK = 1u << 12;      // the default uses the scan-all schedule up to here
 constexpr uint32_t kCscanMinK = (1u << 12) + 1;  // the default uses the cluster scan from here
 constexpr uint32_t kCscanMaxK = 1u << 17;       // ... to here (one register pass per slice)
 // Cluster schedule (rz_cluster.cu); RZ_ERR_UNSUPPORTED when the bitmap slice does not fit in
@@ -116,6 +117,10 @@ constexpr uint32_t kCscanMaxK = 1u << 17;       // ... to here (one register pas
 // Split schedule (rz_produced.cu); RZ_ERR_UNSUPPORTED for k > kFastMaxK or too little shared memory.
 int launch_split(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                  const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
+// Scan-all schedule (rz_produced.cu); RZ_ERR_UNSUPPORTED for k > kFastMaxK, a misaligned list or
+// too little shared memory.
+int launch_scanall(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
+                   const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
                    const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info);
 int cluster_max_block(int w, int items);

@@ -60,6 +60,7 @@ struct ProducedParams {
     unsigned long long* dev_len;
     uint32_t validate;
     uint32_t pdl;                // wait for the preceding (scan) grid before reading candidates
+    uint32_t full_scan;          // scan-all schedule: every CTA reads the whole (16-byte aligned) list
 };
 
 template <int W, int IPT>
@@ -133,9 +134,44 @@ __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(con
     const uint32_t m = s_m;
 
     // ---- the red entries: from the candidates, or (candidates overflowed) from the whole list ---
-    const bool from_cand = m <= p.cand_capacity;
-    const uint32_t scan_n = from_cand ? m : k;
-    for (uint32_t e = threadIdx.x; e < scan_n; e += B) {
+    const bool from_cand = !p.full_scan && m <= p.cand_capacity;
+    if (p.full_scan) {
+        // Scan-all schedule: the list's 16-byte units, four loads in flight per thread (the list
+        // comes from L2 for all but the first CTA to touch a line); the last k % 4 entries below.
+        // The range flag is kept in a register: a global atomic inside the loop could alias the
+        // list for the compiler and serialise the loads.
+        const uint32_t nq = k / 4;
+        const uint4* q4 = reinterpret_cast<const uint4*>(p.idx);
+        bool oor = false;
+#pragma unroll 4
+        for (uint32_t u = threadIdx.x; u < nq; u += B) {
+            const uint4 x = __ldcg(q4 + u);
+            const uint32_t vv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const uint32_t row = vv[c], slot = 4 * u + uint32_t(c);
+                if (row >= n) {
+                    oor = true;
+                } else if (row >= cut) {
+                    const uint32_t v = row - cut;
+                    atomicOr(&mapV[v >> 5], 1u << (v & 31u));
+                    atomicOr(&mapP[slot >> 5], 1u << (slot & 31u));
+                    const uint32_t r = atomicAdd(&s_R, 1u);
+                    if (r < kFastMaxRed) {
+                        u_pos[r] = slot;
+                        u_val[r] = v;
+                    }
+                }
+            }
+        }
+        if (oor) atomicOr(p.status, ST_RANGE);
+    }
+    // Candidates, or the whole list one entry per step (candidates overflowed), or the scan-all
+    // schedule's last k % 4 entries.
+    const uint32_t scan_n = p.full_scan ? (k & 3u) : (from_cand ? m : k);
+    const uint32_t ebase = p.full_scan ? (k & ~3u) : 0u;
+    for (uint32_t e0 = threadIdx.x; e0 < scan_n; e0 += B) {
+        const uint32_t e = ebase + e0;
         uint32_t slot, row;
         if (from_cand) {
             const uint2 c = __ldcg(&p.cand[e]);
@@ -365,6 +401,7 @@ int launch_split(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t
     pp.dev_len = ctx->ws.dev_len;
     pp.validate = validate ? 1u : 0u;
     pp.pdl = 1;
+    pp.full_scan = 0;
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3(grid);
     lc.blockDim = dim3(kProducedBlock);
@@ -381,6 +418,55 @@ int launch_split(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t
         info->block = kProducedBlock;
         info->items = items;
         info->launches += 2;
+    }
+    return RZ_OK;
+}
+
+// Scan-all schedule of rz_remove (RZ_SCHED_SCANALL): the pairing grid alone, each CTA reading the
+// whole list for the red entries. No second grid, no wait of any kind; the cost of the scan grows
+// with k per CTA, so it is the default only for short lists. Needs a 16-byte-aligned list.
+int launch_scanall(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* idx, uint32_t k,
+                   const rz_launch_cfg& cfg, bool validate, cudaStream_t s, LaunchInfo* info) {
+    if (k == 0 || k > kFastMaxK || (reinterpret_cast<uintptr_t>(idx) & 15u)) return RZ_ERR_UNSUPPORTED;
+    const size_t smem = produced_smem_bytes(k);
+    if (smem + 4096 > ctx->smem_optin) return RZ_ERR_UNSUPPORTED;
+    const int items = cfg.items;
+    ProducedFn f = produced_fn(w, items);
+    if (!f) return RZ_ERR_INVALID_ARG;
+    static std::atomic<uint64_t> attr_done[4][4];
+    const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
+    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    if (!(attr_done[wi][ii].load() & bit)) {
+        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              int(ctx->smem_optin) - 4096));
+        attr_done[wi][ii].fetch_or(bit);
+    }
+    const uint32_t tile = uint32_t(kProducedBlock) * uint32_t(items);
+    const uint32_t grid = (k + tile - 1) / tile;
+    ProducedParams pp;
+    pp.data = static_cast<uint8_t*>(data);
+    pp.idx = idx;
+    pp.counts = nullptr;
+    pp.cand_count = ctx->ws.split_count;  // read, not used
+    pp.done = nullptr;
+    pp.cand = nullptr;
+    pp.n = n;
+    pp.k_fixed = k;
+    pp.capacity = k;
+    pp.cand_capacity = 0;
+    pp.status = ctx->ws.status;
+    pp.dev_len = ctx->ws.dev_len;
+    pp.validate = validate ? 1u : 0u;
+    pp.pdl = 0;
+    pp.full_scan = 1;
+    f<<<grid, kProducedBlock, smem, s>>>(pp);
+    RZ_CUDA_TRY(ctx, cudaGetLastError());
+    if (info) {
+        info->grid = int(grid);
+        info->block = kProducedBlock;
+        info->items = items;
+        info->launches += 1;
     }
     return RZ_OK;
 }
@@ -547,6 +633,7 @@ int rz_remove_produced(rz_ctx* ctx, rz_producer* p, void* d_data, uint32_t elem_
     pp.dev_len = ctx->ws.dev_len;
     pp.validate = validate ? 1u : 0u;
     pp.pdl = 0;
+    pp.full_scan = 0;
     f<<<grid, kProducedBlock, smem, s>>>(pp);
     RZ_CUDA_TRY(ctx, cudaGetLastError());
     ctx->last_kernels += 1;

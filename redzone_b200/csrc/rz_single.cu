@@ -155,12 +155,20 @@ int default_cfg(const rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch
     (void)n;
     cfg->use_partition = 0;
     cfg->schedule = RZ_SCHED_AUTO;
-    // Measured on B200 (n = 2^28, L2 flushed): the cluster-scan schedule, which needs no grid-wide
-    // wait, wins from k = 2^13 to 2^17 (7.2 against 11.1 us per call at k = 2^16, graph steady
-    // state); below that the 16-CTA cluster schedule. Where the cluster scan does not run (wider
+    // Measured on B200 (n = 2^28, L2 flushed): up to k = 2^12 the scan-all schedule (one grid, each
+    // CTA reads the whole list: 7.9 against 8.5 us per call at k = 2^10); the cluster-scan schedule,
+    // which needs no grid-wide wait, from k = 2^13 to 2^17 (7.2 against 11.1 us per call at
+    // k = 2^16, graph steady state). Where the cluster scan does not run (wider
     // items at k > 2^16, k > 2^17): the grid schedule with 512-item tiles at 2^15, 1024-item tiles
     // to 2^17 (64 CTAs at 2^16 -- fewer, fuller CTAs shorten the grid-wide wait), and 4096-item
     // tiles on two CTAs per SM beyond.
+    if (k <= kScanAllMaxK) {
+        cfg->block = 256;
+        cfg->items = 1;
+        cfg->ctas_per_sm = 4;  // used only by a fallback (misaligned index list)
+        cfg->schedule = RZ_SCHED_SCANALL;
+        return RZ_OK;
+    }
     if (k >= kCscanMinK && cscan_default_cfg(ctx, k, w, cfg)) return RZ_OK;
     if (k <= kClusterMaxK) {
         cfg->block = 256; cfg->items = 4; cfg->ctas_per_sm = 4;
@@ -206,6 +214,17 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     if (flags & RZ_FORCE_BLOCK) sched = RZ_SCHED_BLOCK;
     if (flags & RZ_FORCE_GRID) sched = RZ_SCHED_GRID;
     if (sched == RZ_SCHED_AUTO) sched = (k <= kClusterMaxK) ? RZ_SCHED_CLUSTER : RZ_SCHED_GRID;
+    if (sched == RZ_SCHED_SCANALL) {
+        LaunchInfo ci;
+        ci.launches = launches;
+        st = launch_scanall(ctx, data, n, w, idx, k, cfg, validate, s, &ci);
+        if (st == RZ_OK) {
+            if (info) *info = ci;
+            return RZ_OK;
+        }
+        if (st != RZ_ERR_UNSUPPORTED) return st;
+        sched = k <= kClusterMaxK ? RZ_SCHED_CLUSTER : RZ_SCHED_GRID;  // misaligned list, or k too large
+    }
     if (sched == RZ_SCHED_SPLIT) {
         LaunchInfo ci;
         ci.launches = launches;

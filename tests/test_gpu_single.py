@@ -71,10 +71,10 @@ def test_widths_and_distributions(ctx, words, dist):
         assert np.array_equal(got[n - k:], host[n - k:]), "tail must be left untouched"
 
 
-SCHEDULES = {"cluster": 2, "grid": 3, "cscan": 4, "split": 5}
+SCHEDULES = {"cluster": 2, "grid": 3, "cscan": 4, "split": 5, "scanall": 6}
 
 
-@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan", "split"])
+@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan", "split", "scanall"])
 def test_every_launch_config_gives_the_same_bits(ctx, sched):
     """The result depends only on (data, idx), never on schedule, block, items or grid."""
     cases = [(1 << 20, 1 << 16, "uniform"), (1 << 18, 1 << 17, "red50"), (1 << 16, 3001, "red100")]
@@ -91,7 +91,7 @@ def test_every_launch_config_gives_the_same_bits(ctx, sched):
                         assert np.array_equal(got[: n - k], exp[: n - k]), (sched, n, k, dist, words, block, items, cps)
 
 
-@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan", "split"])
+@pytest.mark.parametrize("sched", ["cluster", "grid", "cscan", "split", "scanall"])
 @pytest.mark.parametrize("words", [1, 2, 4, 8])
 def test_schedules_on_large_k(ctx, sched, words):
     n = 1 << 21
@@ -152,7 +152,7 @@ def test_n64_every_k_multi_cta(ctx, words):
             exp = expect_of(host, idx)
             for cfg, fl in ((rz.LaunchCfg(32, 1, 4, 0, 3), rz.RZ_FORCE_GRID), (rz.LaunchCfg(32, 2, 4, 0, 3), rz.RZ_FORCE_GRID),
                             (rz.LaunchCfg(32, 1, 4, 0, 4), 0), (rz.LaunchCfg(32, 4, 1, 0, 4), 0),
-                            (rz.LaunchCfg(32, 1, 1, 0, 5), 0)):
+                            (rz.LaunchCfg(32, 1, 1, 0, 5), 0), (rz.LaunchCfg(32, 1, 1, 0, 6), 0)):
                 got = run_gpu(ctx, host, idx, cfg=cfg, flags=fl | rz.RZ_SYNC)
                 assert np.array_equal(got[: n - k], exp[: n - k]), (words, k, rep, cfg)
 
@@ -226,7 +226,7 @@ def test_validation_reports_and_leaves_data_untouched(ctx):
     assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
 
 
-@pytest.mark.parametrize("sched", [4, 5])
+@pytest.mark.parametrize("sched", [4, 5, 6])
 def test_validation_on_the_cluster_scan_and_split_schedules(ctx, sched):
     """A failed validation on the cluster-scan schedule (whose CTAs still meet at every cluster
     barrier phase) or the split schedule (whose pairing CTAs still reset the scan's counter)
@@ -304,7 +304,7 @@ def test_red_list_schedule_around_its_limit(ctx, red, words):
     exp = expect_of(host, idx)
     for cfg in (None, rz.LaunchCfg(256, 4, 1, 0, 3), rz.LaunchCfg(128, 2, 4, 0, 3), rz.LaunchCfg(256, 4, 1, 0, 4),
                 rz.LaunchCfg(128, 2, 4, 0, 4), rz.LaunchCfg(64, 1, 4, 0, 4), rz.LaunchCfg(256, 4, 1, 0, 5),
-                rz.LaunchCfg(256, 1, 1, 0, 5)):
+                rz.LaunchCfg(256, 1, 1, 0, 5), rz.LaunchCfg(256, 1, 1, 0, 6), rz.LaunchCfg(256, 4, 1, 0, 6)):
         got = run_gpu(ctx, host, idx, cfg=cfg)
         assert np.array_equal(got[: n - k], exp[: n - k]), (red, words, cfg)
 
@@ -337,16 +337,18 @@ def test_clobber_flag_is_accepted(ctx):
 
 
 def test_cluster_scan_with_an_unaligned_index_list(ctx):
-    """An index list that does not start on a 16-byte boundary runs on the grid schedule instead
-    (the cluster scan reads it in 16-byte units), with the same result."""
+    """An index list that does not start on a 16-byte boundary runs on another schedule instead
+    (the cluster-scan and scan-all schedules read it in 16-byte units), with the same result."""
     n, k = 1 << 20, 1 << 14
     host = payload(n, 1, seed=4)
     idx = workloads.uniform(n, k, seed=4)
     buf = torch.from_numpy(np.concatenate([[0], idx]).astype(np.int32)).to(DEV)
     d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
-    ctx.remove_cfg(d, buf[1:], rz.LaunchCfg(256, 4, 1, 0, 4), flags=rz.RZ_SYNC)
-    got = d.cpu().numpy().view(np.uint32).reshape(n, 1)
-    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+    for sched in (4, 6):
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        ctx.remove_cfg(d, buf[1:], rz.LaunchCfg(256, 4, 1, 0, sched), flags=rz.RZ_SYNC)
+        got = d.cpu().numpy().view(np.uint32).reshape(n, 1)
+        assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k]), sched
 
 
 def test_partition_more_tiles_than_one_scan_chunk(ctx):
