@@ -13,6 +13,12 @@
 // (rz_pairfill.cuh). k itself is read on the device: the host never waits for the producer.
 // If the candidates overflowed their buffer, each CTA reads the whole list instead (exact,
 // slower); if the list outgrew its capacity, nothing moves and the status says so.
+//
+// The same pairing kernel also serves two schedules of rz_remove on an ordinary index list:
+//   scan-all (RZ_SCHED_SCANALL, the default for short lists): every CTA reads the whole list for
+//     the red entries -- one grid, no wait of any kind;
+//   split (RZ_SCHED_SPLIT): a scan grid lists the red entries as candidates and this kernel runs
+//     as its programmatic dependent, loading its tile while the scan runs.
 #include <algorithm>
 #include <atomic>
 #include <new>
