@@ -70,9 +70,9 @@ typedef enum rz_status {
                             /* programmatic dependent) reads them; no wait inside either grid     */
 #define RZ_SCHED_SCANALL 6  /* one grid, every CTA reads the whole list; no wait (short lists)    */
 
-/* Launch configuration of the single-list kernels (one entry of the 56-point tuning space:
- * block x items x grid scale with the schedule chosen by k, or a cluster-scan launch; plus the
- * Redzone-vs-partition bit). */
+/* Launch configuration of the single-list kernels (one entry of the 63-point tuning space:
+ * block x items x grid scale with the schedule chosen by k, or a cluster-scan, scan-all or split
+ * launch; plus the Redzone-vs-partition bit). */
 typedef struct rz_launch_cfg {
     int32_t block;          /* threads per CTA: 128, 256, 512 or 1024                             */
     int32_t items;          /* items per thread per tile: 1, 2, 4 or 8                            */
@@ -345,8 +345,8 @@ typedef struct rz_tune_entry {
 } rz_tune_entry;
 
 /*
- * Time the 56 launch configurations (48 of block x items x grid scale with the schedule chosen
- * by k, 8 cluster-scan launches of block x items) and the partition path on the caller's data, which every run rewrites (timing does not depend on the
+ * Time the 63 launch configurations (48 of block x items x grid scale with the schedule chosen
+ * by k, 8 cluster-scan, 4 scan-all and 3 split launches) and the partition path on the caller's data, which every run rewrites (timing does not depend on the
  * values). L2 is flushed between repetitions. Writes up to max_out entries sorted by time.
  */
 int rz_autotune_single(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx,
@@ -366,9 +366,9 @@ int rz_tune_table_set_batched(rz_ctx* ctx, uint32_t elem_bytes, const rz_batch_c
 
 /* ---- learned configuration predictor ---------------------------------------------------------- */
 /*
- * A 12 -> 64 -> 64 -> 57 FP32 MLP (ReLU hidden layers) trained and evaluated by the library's
- * own CUDA kernels. Outputs 0..55 are logits over the 56 launch configurations (the order of
- * rz_autotune_single's space), output 56 the logit of "the O(n) partition path is faster". The
+ * A 12 -> 64 -> 64 -> 64 FP32 MLP (ReLU hidden layers) trained and evaluated by the library's
+ * own CUDA kernels. Outputs 0..62 are logits over the 63 launch configurations (the order of
+ * rz_autotune_single's space), output 63 the logit of "the O(n) partition path is faster". The
  * reference has no counterpart: its configuration is fixed at compile time (tests.cu:1-2).
  * Features (rz_mlp_features, computed on the GPU from the index list): log2 n, log2 k, k/n,
  * payload bytes, mean and variance of the log-gap of the sorted 4096-index sample, fraction of
@@ -382,9 +382,9 @@ int  rz_mlp_get_params(rz_mlp* mlp, float* h_params, int32_t count);
 int  rz_mlp_set_params(rz_mlp* mlp, const float* h_params, int32_t count);
 int  rz_mlp_features(rz_ctx* ctx, const uint32_t* d_idx, int64_t n, int64_t k, uint32_t elem_bytes,
                      float* h_features12);
-/* Logits (nsamp x 57) for host features (nsamp x 12). */
+/* Logits (nsamp x 64) for host features (nsamp x 12). */
 int  rz_mlp_forward(rz_mlp* mlp, const float* h_x, int64_t nsamp, float* h_out);
-/* Mean loss and gradient of every parameter over one batch; targets nsamp x 57 (56 probabilities
+/* Mean loss and gradient of every parameter over one batch; targets nsamp x 64 (63 probabilities
  * over configurations + the partition bit). Used to check the kernels against a CPU oracle. */
 int  rz_mlp_gradients(rz_mlp* mlp, const float* h_x, const float* h_t, int64_t nsamp, float* h_grad,
                       float* h_loss);

@@ -1,8 +1,8 @@
 """CPU oracle of the learned predictor -- TEST INFRASTRUCTURE ONLY.
 
-A float64 numpy statement of the network in redzone_b200/csrc/rz_mlp.cu (12 -> 64 -> 64 -> 57,
-ReLU hidden layers; softmax cross-entropy over outputs 0..55 with soft targets plus 0.5 x binary
-cross-entropy of output 56; everything averaged over the batch), with the same flat parameter
+A float64 numpy statement of the network in redzone_b200/csrc/rz_mlp.cu (12 -> 64 -> 64 -> 64,
+ReLU hidden layers; softmax cross-entropy over outputs 0..62 with soft targets plus 0.5 x binary
+cross-entropy of output 63; everything averaged over the batch), with the same flat parameter
 layout, and a statement of the 12 features. Used to check the CUDA forward/backward kernels and
 the feature kernel; the analytic gradient here is itself checked by finite differences in
 tests/test_mlp_oracle.py.
@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-N_IN, N_H, N_OUT, N_CFG = 12, 64, 57, 56
+N_IN, N_H, N_OUT, N_CFG = 12, 64, 64, 63
 BIT_WEIGHT = 0.5
 OFF_W1 = 0
 OFF_B1 = OFF_W1 + N_IN * N_H

@@ -2,9 +2,10 @@
 //
 // The reference fixes its launch configuration at compile time (GPUBlockCount / GPUBlockSize,
 // tests.cu:1-2; prefetch depth 5, redzone.hxx:1134). Here every call can pick its configuration:
-// rz_autotune_single times the 56-point space (block 128/256/512/1024 x items per thread 1/2/4/8
-// x grid scale 1/2/4 with the schedule chosen by k, and eight cluster-scan launches) plus the
-// O(n) partition path with CUDA events and an L2 flush between repetitions; rz_autotune_batched does the same for the batched kernel's tile and grid. The
+// rz_autotune_single times the 63-point space (block 128/256/512/1024 x items per thread 1/2/4/8
+// x grid scale 1/2/4 with the schedule chosen by k, eight cluster-scan, four scan-all and three
+// split launches) plus the O(n) partition path with CUDA events and an L2 flush between
+// repetitions; rz_autotune_batched does the same for the batched kernel's tile and grid. The
 // winners go into a per-context table keyed by (payload width, log2 k) that rz_remove and
 // rz_batch_plan_create consult, and which can be saved to and loaded from a text file.
 #include <algorithm>
@@ -90,9 +91,10 @@ static int ensure_scrub(rz_ctx* ctx) {
     return RZ_OK;
 }
 
-// The space in a fixed order (the predictor's class index is the position here). A cluster-scan
-// point that does not run for an instance (k > 2^17, a slice too long for the block, wide items
-// on 512 threads, a misaligned index list) runs the grid schedule with the same block and items.
+// The space in a fixed order (the predictor's class index is the position here). A cluster-scan,
+// scan-all or split point that does not run for an instance (k > 2^17, a slice too long for the
+// block, wide items on 512 threads, a misaligned index list) runs another schedule (the grid, or
+// the cluster schedule for a short list) with the same block and items.
 void config_space(rz_launch_cfg* out) {
     static const int blocks[4] = {128, 256, 512, 1024};
     static const int items[4] = {1, 2, 4, 8};
@@ -103,6 +105,8 @@ void config_space(rz_launch_cfg* out) {
         for (int i : items)
             for (int g : gs) out[q++] = rz_launch_cfg{b, i, g, 0, RZ_SCHED_AUTO};
     for (const auto& c : cscan) out[q++] = rz_launch_cfg{c[0], c[1], 2, 0, RZ_SCHED_CSCAN};
+    for (int i : {1, 2, 4, 8}) out[q++] = rz_launch_cfg{256, i, 2, 0, RZ_SCHED_SCANALL};
+    for (int i : {1, 2, 4}) out[q++] = rz_launch_cfg{256, i, 2, 0, RZ_SCHED_SPLIT};
 }
 
 }  // namespace rz

@@ -348,9 +348,7 @@ int rz_remove(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const u
     cudaSetDevice(ctx->device);
     rz_launch_cfg cfg{};
     bool have = false;
-    // The predictor's configuration space does not hold the scan-all schedule, which is faster than
-    // all of it for short lists: there the default stands.
-    if ((flags & RZ_USE_PREDICTOR) && uint64_t(k) > kScanAllMaxK)
+    if (flags & RZ_USE_PREDICTOR)
         have = predict_cfg(ctx, uint32_t(n), uint32_t(k), elem_bytes, d_idx,
                               reinterpret_cast<cudaStream_t>(stream), &cfg);
     if (!have) have = tuned_cfg(ctx, uint32_t(n), uint32_t(k), elem_bytes, &cfg);

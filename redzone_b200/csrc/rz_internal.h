@@ -126,8 +126,9 @@ int launch_cluster(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
 int cluster_max_block(int w, int items);
 constexpr uint32_t kClusterMaxK = 1u << 14;  // RZ_SCHED_AUTO uses the cluster schedule up to here
 // The launch-configuration space in its canonical order (rz_autotune.cpp): 48 grid / cluster
-// points (block x items x grid scale, schedule chosen by k) and 8 cluster-scan points.
-constexpr int kConfigSpace = 56;
+// points (block x items x grid scale, schedule chosen by k), 8 cluster-scan, 4 scan-all and 3
+// split points.
+constexpr int kConfigSpace = 63;
 void config_space(rz_launch_cfg* out);
 int launch_validate(rz_ctx* ctx, uint32_t n, const uint32_t* idx, uint32_t k, cudaStream_t s);
 // rz_keep: gather data[keep[j]] into `stage` (m items), then copy the stage to data[0..m).

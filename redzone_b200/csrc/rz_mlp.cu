@@ -1,8 +1,8 @@
 // rz_mlp.cu -- learned launch-configuration predictor: features, FP32 MLP training and inference.
 //
-// The network maps 12 features of a removal instance to 56 logits (softmax over the launch
+// The network maps 12 features of a removal instance to 63 logits (softmax over the launch
 // configurations of config_space(), rz_autotune.cpp) plus one logit for "the O(n) partition
-// path beats Redzone". Layers: 12 -> 64 (ReLU) -> 64 (ReLU) -> 57. All arithmetic is FP32 in
+// path beats Redzone". Layers: 12 -> 64 (ReLU) -> 64 (ReLU) -> 64. All arithmetic is FP32 in
 // hand-written kernels (no cuBLAS): one warp per sample for the forward and backward passes
 // with the weights staged in shared memory, one thread per parameter for the weight gradients
 // and the Adam update. Training targets are the kernels' own timings (soft targets favouring
@@ -34,7 +34,7 @@ constexpr int kOffW2 = kOffB1 + kH;
 constexpr int kOffB2 = kOffW2 + kH * kH;
 constexpr int kOffW3 = kOffB2 + kH;
 constexpr int kOffB3 = kOffW3 + kH * kOut;
-constexpr int kParams = kOffB3 + kOut;  // 8697
+constexpr int kParams = kOffB3 + kOut;  // 9152
 constexpr int kSample = 4096;
 constexpr float kBitWeight = 0.5f;  // weight of the partition-bit loss
 

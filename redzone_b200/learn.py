@@ -6,7 +6,7 @@ Pipeline (``python -m redzone_b200.learn collect|train|eval``):
 * ``collect``: seeded removal instances drawn as mixes of the two single-list benchmark
   configurations (n = 2^20 and n = 2^28, plus intermediate sizes; int32 and 16-byte payloads;
   uniform, clustered and tail-heavy indices). For each: the 12 features from the GPU feature
-  kernel (``rz_mlp_features``) and the time of every one of the 56 launch configurations plus the
+  kernel (``rz_mlp_features``) and the time of every one of the 63 launch configurations plus the
   partition path (``rz_autotune_single``, CUDA events, L2 flushed between runs).
 * ``train``: soft targets (configurations within a few percent of the fastest get most of the
   mass) and the partition bit; Adam on the GPU through ``rz_mlp_train``.
@@ -32,8 +32,8 @@ import numpy as np
 from . import _native
 from ._native import LaunchCfg
 
-N_IN, N_OUT, N_CFG = 12, 57, 56
-SCHED_AUTO, SCHED_CSCAN = 0, 4
+N_IN, N_OUT, N_CFG = 12, 64, 63
+SCHED_AUTO, SCHED_CSCAN, SCHED_SPLIT, SCHED_SCANALL = 0, 4, 5, 6
 DATA = Path(__file__).resolve().parent / "data"
 _FP = ctypes.POINTER(ctypes.c_float)
 
@@ -44,11 +44,14 @@ def _fp(a: np.ndarray):
 
 def config_space() -> list[tuple[int, int, int, int]]:
     """(block, items, grid scale, schedule) in the library's canonical order (class index =
-    position): 48 points with the schedule chosen by k, then 8 cluster-scan launches."""
+    position): 48 points with the schedule chosen by k, then 8 cluster-scan, 4 scan-all and 3
+    split launches."""
     grid = [(b, i, g, SCHED_AUTO) for b in (128, 256, 512, 1024) for i in (1, 2, 4, 8) for g in (1, 2, 4)]
     cscan = [(b, i, 2, SCHED_CSCAN) for b, i in ((128, 2), (128, 4), (256, 1), (256, 2), (256, 4), (256, 8),
                                                   (512, 2), (512, 4))]
-    return grid + cscan
+    scanall = [(256, i, 2, SCHED_SCANALL) for i in (1, 2, 4, 8)]
+    split = [(256, i, 2, SCHED_SPLIT) for i in (1, 2, 4)]
+    return grid + cscan + scanall + split
 
 
 class Mlp:
@@ -133,7 +136,7 @@ def attach_default(ctx) -> Mlp | None:
 
 # ---- training data ------------------------------------------------------------------------------
 def soft_targets(times: np.ndarray, tau: float = 0.03) -> np.ndarray:
-    """times: (N, 57) ms for the 56 configurations and the partition path -> (N, 57) targets."""
+    """times: (N, 64) ms for the 63 configurations and the partition path -> (N, 64) targets."""
     t = np.asarray(times, np.float64)
     cfg = t[:, :N_CFG]
     best = cfg.min(1, keepdims=True)
@@ -165,7 +168,7 @@ def draw_instance(rng: np.random.Generator) -> tuple[int, int, int, str]:
 
 
 def collect(ctx, count: int, seed: int, reps: int = 1, log_every: int = 500):
-    """Features and 57 timings for `count` seeded instances (timing rewrites a scratch array)."""
+    """Features and 64 timings for `count` seeded instances (timing rewrites a scratch array)."""
     import torch
     from . import workloads
 
@@ -211,7 +214,7 @@ def default_class(ctx, n, k, w) -> int:
         return space.index(key)
     # The default's block may be clamped; pick the nearest class of the same schedule family with
     # the same items and grid.
-    fam = SCHED_CSCAN if c.schedule == SCHED_CSCAN else SCHED_AUTO
+    fam = c.schedule if c.schedule in (SCHED_CSCAN, SCHED_SPLIT, SCHED_SCANALL) else SCHED_AUTO
     return min(range(N_CFG), key=lambda q: (space[q][3] != fam, space[q][1] != c.items,
                                             space[q][2] != c.ctas_per_sm, abs(space[q][0] - c.block)))
 

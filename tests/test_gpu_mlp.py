@@ -70,7 +70,7 @@ def test_feature_kernel_matches_cpu_oracle(ctx, dist, n, k, w):
 def test_training_on_the_gpu_learns_a_separable_task(ctx):
     rng = np.random.default_rng(0)
     x = rng.uniform(0, 1, (4000, 12)).astype(np.float32)
-    label = (x[:, 0] * 7).astype(int) * 8 + (x[:, 1] * 8).astype(int)  # 56 classes on a grid
+    label = (x[:, 0] * 7).astype(int) * 9 + (x[:, 1] * 9).astype(int)  # 63 classes on a grid
     t = np.zeros((4000, mlp_ref.N_OUT), np.float32)
     t[np.arange(4000), label] = 1.0
     t[:, mlp_ref.N_CFG] = (x[:, 2] > 0.5)

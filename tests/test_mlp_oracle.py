@@ -60,7 +60,7 @@ def _regret(cls, T):
 
 
 def test_shipped_predictor_beats_the_method_without_it():
-    """Held-out seeds, timings of all 56 configurations + partition measured on a B200 (median of
+    """Held-out seeds, timings of all 63 configurations + partition measured on a B200 (median of
     5 runs each): the network's choice is within 5 % of the exhaustive best on average, and better
     than the fixed default configuration and than the best single configuration for all inputs."""
     p = np.load(WEIGHTS)["params"].astype(np.float64)
