@@ -328,6 +328,20 @@ __global__ void __launch_bounds__(256) split_scan_kernel(const uint32_t* __restr
     if (__any_sync(0xffffffffu, oor) && lane == 0) atomicOr(status, ST_RANGE);
 }
 
+// Let the pairing kernel for (w, items) use the device's large shared memory; once per device.
+static int allow_produced_smem(rz_ctx* ctx, ProducedFn f, uint32_t w, int items) {
+    static std::atomic<uint64_t> done[4][4];
+    const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
+    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
+    const uint64_t bit = 1ull << (ctx->device & 63);
+    if (!(done[wi][ii].load() & bit)) {
+        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              int(ctx->smem_optin) - 4096));
+        done[wi][ii].fetch_or(bit);
+    }
+    return RZ_OK;
+}
+
 // The library's own producer: every row i < n with keys[i] < threshold. Each thread reads 16
 // keys per step (four 16-byte loads in flight: a 4-byte load per step would leave the kernel
 // waiting on memory latency) and emits them warp-wide; keys not 16-byte aligned, and the last
@@ -373,15 +387,8 @@ int launch_split(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t
     int items = cfg.items;
     ProducedFn f = produced_fn(w, items);
     if (!f) return RZ_ERR_INVALID_ARG;
-    static std::atomic<uint64_t> attr_done[4][4];
-    const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
-    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
-    const uint64_t bit = 1ull << (ctx->device & 63);
-    if (!(attr_done[wi][ii].load() & bit)) {
-        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              int(ctx->smem_optin) - 4096));
-        attr_done[wi][ii].fetch_or(bit);
-    }
+    const int ast = allow_produced_smem(ctx, f, w, items);
+    if (ast != RZ_OK) return ast;
     const uint32_t vec = (reinterpret_cast<uintptr_t>(idx) & 15u) == 0 ? 1u : 0u;
     const uint32_t units = vec ? k / 4 + (k & 3u) : k;
     const uint32_t sgrid = std::max<uint32_t>(1u, std::min<uint32_t>((units + 255) / 256, uint32_t(ctx->sms) * 4));
@@ -439,15 +446,8 @@ int launch_scanall(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     const int items = cfg.items;
     ProducedFn f = produced_fn(w, items);
     if (!f) return RZ_ERR_INVALID_ARG;
-    static std::atomic<uint64_t> attr_done[4][4];
-    const int wi = w == 4 ? 0 : w == 8 ? 1 : w == 16 ? 2 : 3;
-    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
-    const uint64_t bit = 1ull << (ctx->device & 63);
-    if (!(attr_done[wi][ii].load() & bit)) {
-        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              int(ctx->smem_optin) - 4096));
-        attr_done[wi][ii].fetch_or(bit);
-    }
+    const int ast = allow_produced_smem(ctx, f, w, items);
+    if (ast != RZ_OK) return ast;
     const uint32_t tile = uint32_t(kProducedBlock) * uint32_t(items);
     const uint32_t grid = (k + tile - 1) / tile;
     ProducedParams pp;
@@ -613,15 +613,8 @@ int rz_remove_produced(rz_ctx* ctx, rz_producer* p, void* d_data, uint32_t elem_
     ProducedFn f = produced_fn(elem_bytes, items);
     if (!f) return RZ_ERR_INVALID_ARG;
     const size_t smem = produced_smem_bytes(p->capacity);
-    static std::atomic<uint64_t> attr_done[4][4];
-    const int wi = elem_bytes == 4 ? 0 : elem_bytes == 8 ? 1 : elem_bytes == 16 ? 2 : 3;
-    const int ii = items == 1 ? 0 : items == 2 ? 1 : items == 4 ? 2 : 3;
-    const uint64_t bit = 1ull << (ctx->device & 63);
-    if (!(attr_done[wi][ii].load() & bit)) {
-        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              int(ctx->smem_optin) - 4096));
-        attr_done[wi][ii].fetch_or(bit);
-    }
+    st = allow_produced_smem(ctx, f, elem_bytes, items);
+    if (st != RZ_OK) return st;
     const uint32_t tile = uint32_t(kProducedBlock) * uint32_t(items);
     const uint32_t grid = std::max<uint32_t>(1u, (p->capacity + tile - 1) / tile);
     ProducedParams pp;
