@@ -351,6 +351,9 @@ typedef struct rz_tune_entry {
  */
 int rz_autotune_single(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx,
                        int64_t k, int32_t reps, rz_tune_entry* out, int32_t max_out, int32_t* count);
+/* The launch-configuration space in its canonical order (the predictor's class index is the
+ * position): writes up to max entries, returns the size of the space. Host only, no GPU needed. */
+int rz_config_space(rz_launch_cfg* out, int32_t max);
 /* Time candidate batched configurations on `lists`; *best receives the fastest. */
 int rz_autotune_batched(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
                         int32_t reps, rz_batch_cfg* best, float* best_ms);

@@ -115,6 +115,13 @@ using namespace rz;
 
 extern "C" {
 
+int rz_config_space(rz_launch_cfg* out, int32_t max) {
+    rz_launch_cfg space[kConfigSpace];
+    config_space(space);
+    for (int q = 0; q < kConfigSpace && q < max && out; ++q) out[q] = space[q];
+    return kConfigSpace;
+}
+
 int rz_autotune_single(rz_ctx* ctx, void* d_data, int64_t n, uint32_t w, const uint32_t* d_idx, int64_t k,
                        int32_t reps, rz_tune_entry* out, int32_t max_out, int32_t* count) {
     if (!ctx || !out || max_out < 1 || reps < 1) return RZ_ERR_INVALID_ARG;

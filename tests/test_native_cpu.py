@@ -78,3 +78,15 @@ def test_device_producer_header_compiles_in_a_caller_kernel(tmp_path):
                         str(tmp_path / "caller.o"), "-I", os.path.join(root, "include")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_predictor_space_matches_the_library():
+    """The predictor's class index is a position in the library's configuration space: the Python
+    mirror used for training and evaluation must list the same configurations in the same order."""
+    from redzone_b200 import learn
+    n = _native.lib.rz_config_space(None, 0)
+    out = (_native.LaunchCfg * n)()
+    assert _native.lib.rz_config_space(out, n) == n == learn.N_CFG
+    lib = [(c.block, c.items, c.ctas_per_sm, c.schedule) for c in out]
+    assert lib == learn.config_space()
+    assert all(c.use_partition == 0 for c in out)
