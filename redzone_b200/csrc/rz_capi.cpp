@@ -403,7 +403,7 @@ int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, cons
     int st = check_args(d_data, n, elem_bytes, d_idx, k);
     if (st != RZ_OK) return st;
     if (new_len) *new_len = n - k;
-    rz_launch_cfg cfg{256, 8, 1, 1};
+    rz_launch_cfg cfg{256, 8, 1, 1, RZ_SCHED_AUTO};
     return rz_remove_cfg(ctx, d_data, n, elem_bytes, d_idx, k, &cfg, flags | RZ_FORCE_PARTITION, stream);
 }
 

@@ -130,8 +130,6 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
     const uint32_t t = blockIdx.x;  // this CTA's tile (none when t >= ntiles)
     const uint32_t chunk_base = min(t, ntiles) * TILE;
     const uint32_t kw = (k + 31) >> 5;
-    const int E = IPT * nw;
-    const uint32_t lt = lanemask_lt();
 
     extern __shared__ __align__(16) uint32_t s_dyn[];
     __shared__ uint32_t s_cnt[2][16 * 16 + 1];
