@@ -113,3 +113,55 @@ def test_batched_oracle_equals_per_list():
         seg = data2[data_off[l]: data_off[l] + n[l]]
         oracle.remove(seg, idx[idx_off[l]: idx_off[l] + k[l]])
     assert np.array_equal(data, data2)
+
+
+def _remove_via_red_entries(a, idx):
+    """The formulation the cluster-scan, scan-all, split and produced-list kernels implement,
+    restated in numpy: only the red entries (i, idx[i] >= cut) matter. V = {idx[i] - cut}, P = {i};
+    a hole idx[i] < cut takes tail item i unless i is in V, in which case it is a destination
+    orphan (V \\ P, ranked by position) and takes the tail item of the source orphan (P \\ V,
+    ranked by position) of the same rank."""
+    n, k = a.shape[0], idx.size
+    cut = n - k
+    out = a.copy()
+    if k == 0 or k == n:
+        return out
+    idx = idx.astype(np.int64)
+    red = idx >= cut
+    V = np.zeros(k, bool)
+    V[idx[red] - cut] = True
+    P = red
+    src_orphans = np.flatnonzero(P & ~V)          # positions, ascending
+    dst_rank = np.cumsum(V & ~P) - 1               # rank of each destination orphan
+    tail = a[cut:].copy()
+    for i in range(k):
+        if P[i]:
+            continue
+        if not V[i]:
+            out[idx[i]] = tail[i]
+        else:
+            out[idx[i]] = tail[src_orphans[dst_rank[i]]]
+    return out
+
+
+@pytest.mark.parametrize("dist", ["uniform", "clustered", "tail", "red0", "red50", "red100"])
+def test_red_entry_formulation_equals_the_canonical_rule(dist):
+    rng = np.random.default_rng(["uniform", "clustered", "tail", "red0", "red50", "red100"].index(dist))
+    cases = 0
+    for _ in range(200):
+        n = int(rng.integers(2, 4000))
+        k = int(rng.integers(1, n))
+        if dist == "tail" and k > n // 10:
+            continue
+        if dist.startswith("red") and k - (k * int(dist[3:])) // 100 > n - k:
+            continue
+        if dist == "clustered" and k < 256:
+            continue
+        idx = workloads.make(dist, n, k, int(rng.integers(0, 1 << 30)))
+        a = rng.integers(0, 1 << 31, size=(n, 2), dtype=np.int64).astype(np.uint32)
+        expect = a.copy()
+        oracle.remove(expect, idx)
+        got = _remove_via_red_entries(a, idx)
+        assert np.array_equal(got[: n - k], expect[: n - k]), (dist, n, k)
+        cases += 1
+    assert cases > 20
