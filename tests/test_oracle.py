@@ -149,10 +149,8 @@ def test_red_entry_formulation_equals_the_canonical_rule(dist):
     rng = np.random.default_rng(["uniform", "clustered", "tail", "red0", "red50", "red100"].index(dist))
     cases = 0
     for _ in range(200):
-        n = int(rng.integers(2, 4000))
-        k = int(rng.integers(1, n))
-        if dist == "tail" and k > n // 10:
-            continue
+        n = int(rng.integers(20, 4000))
+        k = int(rng.integers(1, max(2, n // 10))) if dist == "tail" else int(rng.integers(1, n))
         if dist.startswith("red") and k - (k * int(dist[3:])) // 100 > n - k:
             continue
         if dist == "clustered" and k < 256:
