@@ -239,7 +239,9 @@ int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
 int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
                       int64_t* new_len, rz_stream_t stream);
 
-/* The configuration rz_remove would choose for (n, k, elem_bytes) without a predictor. */
+/* The configuration rz_remove would choose for (n, k, elem_bytes) without a predictor or tuning
+ * table: the scan-all schedule up to k = 2^12, the cluster scan up to 2^17 (where it runs), the
+ * grid schedule beyond. */
 int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
                    rz_launch_cfg* cfg);
 
@@ -346,8 +348,9 @@ typedef struct rz_tune_entry {
 
 /*
  * Time the 63 launch configurations (48 of block x items x grid scale with the schedule chosen
- * by k, 8 cluster-scan, 4 scan-all and 3 split launches) and the partition path on the caller's data, which every run rewrites (timing does not depend on the
- * values). L2 is flushed between repetitions. Writes up to max_out entries sorted by time.
+ * by k, 8 cluster-scan, 4 scan-all and 3 split launches) and the partition path on the caller's
+ * data, which every run rewrites (timing does not depend on the values). L2 is flushed between
+ * repetitions. Writes up to max_out entries sorted by time.
  */
 int rz_autotune_single(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx,
                        int64_t k, int32_t reps, rz_tune_entry* out, int32_t max_out, int32_t* count);
