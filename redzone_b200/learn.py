@@ -1,7 +1,7 @@
 """Learned launch-configuration predictor: data from the kernels' own timings, GPU training,
 regret against exhaustive autotuning.
 
-Pipeline (``python -m redzone_b200.learn collect|train|eval``):
+Pipeline (``python -m redzone_b200.learn collect|train``; ``train`` also evaluates):
 
 * ``collect``: seeded removal instances drawn as mixes of the two single-list benchmark
   configurations (n = 2^20 and n = 2^28, plus intermediate sizes; int32 and 16-byte payloads;
@@ -10,9 +10,10 @@ Pipeline (``python -m redzone_b200.learn collect|train|eval``):
   partition path (``rz_autotune_single``, CUDA events, L2 flushed between runs).
 * ``train``: soft targets (configurations within a few percent of the fastest get most of the
   mass) and the partition bit; Adam on the GPU through ``rz_mlp_train``.
-* ``eval``: on held-out seeds, regret = time of the predicted configuration / time of the best
-  one - 1 (the exhaustive autotune table is the judge); compared with the fixed default
-  configuration (``rz_default_cfg``), i.e. the method without the network.
+* evaluation (end of ``train``): on held-out seeds, regret = time of the predicted
+  configuration / time of the best one - 1 (the exhaustive autotune table is the judge);
+  compared with the fixed default configuration (``rz_default_cfg``), i.e. the method without
+  the network.
 
 ``Mlp`` wraps the C-ABI network; ``attach_default(ctx)`` loads the shipped weights
 (``redzone_b200/data/predictor.npz``) into a context for ``rz_remove(..., RZ_USE_PREDICTOR)``.
