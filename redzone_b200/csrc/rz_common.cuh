@@ -144,7 +144,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
         asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
 }
 
-// ---- mbarrier + 1-D TMA bulk copies (no multicast) ---------------------------------------------
+// ---- mbarrier + 1-D TMA bulk copies (each into its own CTA only) ---------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
