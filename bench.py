@@ -46,13 +46,14 @@ METRIC = "items removed/s"
 UNIT = "items/s"
 
 
-def config(parallelism: str) -> dict:
+def config(world: int) -> dict:
+    """The workload of both arms (the reference arm prints the same object)."""
     return {
         "workload": f"single-list Redzone removal, n=2^{N_LOG2} int32 payload (iota), k=2^{K_LOG2} distinct "
                     f"uniform unsorted indices",
         "n": 1 << N_LOG2, "k": 1 << K_LOG2, "elem_bytes": W_BYTES, "distribution": "uniform",
         "l2": "flushed between timed steps (256 MiB scrub write)", "index_sets": NSETS,
-        "parallelism": parallelism,
+        "parallelism": "single GPU" if world == 1 else f"{world} independent replicas (one list per GPU)",
     }
 
 
@@ -122,11 +123,6 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init(args):
-    from redzone_b200 import dist
-    return dist.env_ranks()
-
-
 def alg_bytes(n: int, k: int, w: int, idx: np.ndarray) -> float:
     """Algorithmic bytes of one Redzone call: read R, read surviving tail items, write the holes,
     write + read the k-bit red-zone bitmap: 4k + 2w(k - k_r) + k/4, k_r = #{R >= n-k}."""
@@ -135,11 +131,22 @@ def alg_bytes(n: int, k: int, w: int, idx: np.ndarray) -> float:
 
 
 # ------------------------------------------------------------------------------------------------
+def load_workloads():
+    """``redzone_b200/workloads.py`` (plain numpy) loaded by its path. Importing it through the
+    package would also load the package's CUDA library, which the CPU legs must not touch."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_rz_bench_workloads", ROOT / "redzone_b200" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def cpu_reference_time(n: int, k: int, steps: int, warmup: int, time_budget_s: float):
     """Time the reference's redzone_CPU (oracle/_ref) -- or the oracle port if it is absent."""
     import oracle
-    from redzone_b200 import workloads
 
+    workloads = load_workloads()
     a = np.arange(n, dtype=np.int32)
     sets = [workloads.uniform(n, k, seed=s).astype(np.int32) for s in range(NSETS)]
     L = oracle.ref_lib()
@@ -170,23 +177,72 @@ def cpu_reference_time(n: int, k: int, steps: int, warmup: int, time_budget_s: f
     return kind, cores, times
 
 
+def cpu_par_remove_time(n: int, k: int, max_calls: int, time_budget_s: float):
+    """Time the reference's O(n) CPU comparator -- mark with -1, then std::remove(par_unseq)
+    (std_parallel_remove.hxx:13-36, compiled into oracle/_ref) -- on the same workload. The list
+    is restored to iota before each call (outside the timer). None when oracle/_ref is absent."""
+    import oracle
+
+    L = oracle.ref_lib()
+    if L is None:
+        return None
+    workloads = load_workloads()
+    iota = np.arange(n, dtype=np.int32)
+    a = iota.copy()
+    sets = [workloads.uniform(n, k, seed=s).astype(np.int32) for s in range(NSETS)]
+    times = []
+    t_start = time.perf_counter()
+    for i in range(max_calls + 1):  # the first call is a warm-up
+        np.copyto(a, iota)
+        r = sets[i % NSETS]
+        t0 = time.perf_counter()
+        L.ref_par_remove(a.ctypes.data, n, r.ctypes.data, k)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            times.append(dt)
+        if time.perf_counter() - t_start > time_budget_s and len(times) >= 1:
+            break
+    parallel = int(L.ref_pstl_parallel())
+    mean = statistics.mean(times)
+    return {"value": k / mean, "unit": UNIT, "ms_per_call": mean * 1e3, "calls": len(times),
+            "cores": 1 if not parallel else int(L.ref_redzone_threads()) + 1,
+            "pstl_parallel_backend": bool(parallel),
+            "note": "libstdc++ runs std::remove(par_unseq) serially without oneTBB, which this host lacks"
+                    if not parallel else "libstdc++ parallel backend present"}
+
+
+def cpu_baselines(n: int, k: int, steps: int, warmup: int, budget_s: float, par_calls: int):
+    """Both of the reference's CPU paths on this workload: redzone_CPU (the reported baseline, its
+    figure is `value`) and std::remove(par_unseq) beside it."""
+    kind, cores, times = cpu_reference_time(n, k, steps, warmup, budget_s)
+    mean = statistics.mean(times)
+    rz_cpu = {"value": k / mean, "unit": UNIT, "ms_per_call": mean * 1e3, "calls": len(times), "cores": cores,
+              "kind": kind}
+    par = cpu_par_remove_time(n, k, par_calls, budget_s)
+    host = {"hardware_threads": os.cpu_count(), "tbb": "project TBB-API shim (oneTBB not installed)"}
+    return kind, cores, times, rz_cpu, par, host
+
+
 def reference_arm(args):
-    world, rank, _ = dist_init(args)
+    # The rank comes from the launcher's environment: this arm loads none of the package's code.
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     n, k = 1 << N_LOG2, 1 << K_LOG2
-    kind, cores, times = cpu_reference_time(n, k, args.steps, args.warmup, time_budget_s=120.0)
+    kind, cores, times, rz_cpu, par, host = cpu_baselines(n, k, args.steps, args.warmup, 120.0, par_calls=5)
     mean = statistics.mean(times)
     v = k / mean
     line = {
-        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": len(times),
         "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "impl": "reference",
-        "config": config("host CPU, reference redzone_CPU"),
+        "config": config(world),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{len(times)} full calls of the workload (n=2^{N_LOG2}, k=2^{K_LOG2}); "
-                                   f"removal list restored before each call (the reference clobbers it)"},
+                         "sample": f"{len(times)} full calls of the workload (n=2^{N_LOG2}, k=2^{K_LOG2}) through "
+                                   f"the reference's redzone_CPU; removal list restored before each call (the "
+                                   f"reference clobbers it)",
+                         "redzone_cpu": rz_cpu, "std_remove_par": par, "host": host},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -316,16 +372,18 @@ def own_arm(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        kind, cores, times = cpu_reference_time(n, k, steps=50, warmup=2, time_budget_s=20.0)
+        kind, cores, times, rz_cpu, par, host = cpu_baselines(n, k, 50, 2, 20.0, par_calls=3)
         cpu = {"value": k / statistics.mean(times), "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": f"{len(times)} full calls of the same workload (n=2^{N_LOG2}, k=2^{K_LOG2}) on the host"}
+               "sample": f"{len(times)} full calls of the same workload (n=2^{N_LOG2}, k=2^{K_LOG2}) on the host "
+                         f"through the reference's redzone_CPU",
+               "redzone_cpu": rz_cpu, "std_remove_par": par, "host": host}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": config("single GPU" if world == 1 else f"{world} independent replicas (one list per GPU)"),
+            "config": config(world),
             "timed_region_ms": region_ms,
             "gpu_launches": args.steps * kernels_per_call,
             "launch": {"grid": grid, "block": block, "kernels_per_call": kernels_per_call},

@@ -233,11 +233,20 @@ int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
  * scratch is a fixed device-global array of about 8.4 MB that every GPU loading this library
  * holds until exit. Limits: k <= 2^20 (RZ_ERR_UNSUPPORTED above that), n < 2^32. The first call
  * on a device, with that device current, looks up the array's address: make it before any stream
- * capture. Calls share the array, so calls that overlap on the GPU race; order them on one
- * stream. Asynchronous on `stream`; same result as rz_remove; no RZ_VALIDATE.
+ * capture, and do not use the library on a device after a cudaDeviceReset. `stream` must belong
+ * to the current device (RZ_ERR_INVALID_ARG otherwise). Calls share the array, so calls that
+ * overlap on the GPU race; order them on one stream. Asynchronous on `stream`; same result as
+ * rz_remove; no RZ_VALIDATE. Errors found on the device (an index >= n, which is skipped; a
+ * bounded wait that gave up) are collected in the array and read with rz_noalloc_sync_status.
  */
 int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
                       int64_t* new_len, rz_stream_t stream);
+/* Companion of rz_remove_noalloc (no counterpart in the reference): synchronise `stream` (on the
+ * current device), then return and clear the device-side status of every rz_remove_noalloc call on
+ * this device since the last rz_noalloc_sync_status -- RZ_ERR_OUT_OF_RANGE, RZ_ERR_TIMEOUT,
+ * RZ_ERR_DUPLICATE (inconsistent orphan counts, only from invalid input) or RZ_OK. Allocates
+ * nothing. */
+int rz_noalloc_sync_status(rz_stream_t stream);
 
 /* The configuration rz_remove would choose for (n, k, elem_bytes) without a predictor or tuning
  * table: the scan-all schedule up to k = 2^12, the cluster scan up to 2^17 (where it runs), the

@@ -14,6 +14,7 @@ calls it.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -27,9 +28,17 @@ _oracle = None
 _ref = None
 
 
+# Where the reference checkout is read from when oracle/_ref is built (environment variable
+# RZ_REFERENCE_DIR overrides it); machines without it keep a prebuilt oracle/_ref.
+REFERENCE_DIR = os.environ.get("RZ_REFERENCE_DIR", "/root/reference")
+
+
 def build(ref: bool = True) -> None:
     """Compile the oracle (and the reference CPU path when its sources are present)."""
-    subprocess.run(["make", "-s", "-C", str(HERE), "oracle"] + (["ref"] if ref else []), check=True)
+    args = ["make", "-s", "-C", str(HERE), "oracle"]
+    if ref:
+        args += ["ref", f"REF={REFERENCE_DIR}"]
+    subprocess.run(args, check=True)
 
 
 def _vp(a: np.ndarray) -> ctypes.c_void_p:

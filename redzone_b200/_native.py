@@ -105,6 +105,7 @@ _sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchC
 _sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
 _sig("rz_last_launch", c_i32, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)])
 _sig("rz_remove_noalloc", c_i32, [c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_vp])
+_sig("rz_noalloc_sync_status", c_i32, [c_vp])
 _sig("rz_config_space", c_i32, [ctypes.POINTER(LaunchCfg), c_i32])
 _sig("rz_producer_create", c_i32, [c_vp, c_i64, c_i64, ctypes.POINTER(c_vp)])
 _sig("rz_producer_destroy", None, [c_vp])

@@ -34,11 +34,12 @@ def _headers():
         (ROOT / "include").glob("*.h*"))
 
 
-def _compile(src: Path, verbose: bool) -> Path:
+def _compile(src: Path, verbose: bool) -> tuple[Path, bool]:
+    """Compile one source; returns (object, whether it was rebuilt)."""
     obj = OBJ_DIR / (src.name + ".o")
     newest_dep = max([src.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
     if obj.exists() and obj.stat().st_mtime >= newest_dep:
-        return obj
+        return obj, False
     cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cpp":
         cmd[1:1] = ["-x", "cu"]
@@ -49,20 +50,29 @@ def _compile(src: Path, verbose: bool) -> Path:
         raise RuntimeError(f"nvcc failed for {src.name}:\n{res.stdout}\n{res.stderr}")
     if verbose and res.stderr:
         sys.stderr.write(res.stderr)
-    return obj
+    return obj, True
 
 
-def build(verbose: bool = False) -> Path:
+def build(verbose: bool = False, quiet: bool = False) -> Path:
+    """Compile what is out of date and link; prints which sources were rebuilt and whether the
+    library was relinked (unless quiet)."""
     OBJ_DIR.mkdir(parents=True, exist_ok=True)
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
+        done = list(ex.map(lambda s: _compile(s, verbose), srcs))
+    objs = [o for o, _ in done]
+    rebuilt = [s.name for s, (_, r) in zip(srcs, done) if r]
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
+        if not quiet:
+            print(f"redzone_b200: {LIB.name} up to date ({len(srcs)} sources, none rebuilt)")
         return LIB
     cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcuda"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    if not quiet:
+        print(f"redzone_b200: rebuilt {len(rebuilt)} of {len(srcs)} sources "
+              f"({', '.join(rebuilt) if rebuilt else 'objects newer than the library'}); linked {LIB.name}")
     return LIB
 
 

@@ -146,6 +146,8 @@ bool predict_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, const uint32_t
                  cudaStream_t s, rz_launch_cfg* cfg);
 bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
 void release_extras(rz_ctx* ctx);
+// Map device status bits (ST_* of rz_common.cuh) to an rz_status code, most severe first.
+int map_status(uint32_t bits);
 // Wait for the stream, then map the device status to rz_status (clearing it); with new_len, also
 // read back the device-tracked length of the last call.
 int read_status(rz_ctx* ctx, cudaStream_t s, int64_t* new_len = nullptr);

@@ -16,13 +16,18 @@
 //   * Set-up: the first call on a device, with that device current, looks up the array's device
 //     address (cudaGetSymbolAddress) and caches it. Make that first call before any stream
 //     capture on that device.
+//   * The stream must belong to the current device (checked); a cudaDeviceReset discards the
+//     array's address, so this library must not be used on a device after it was reset.
 //   * All calls share the one array and it keeps the last call's contents. Each call clears, on
 //     its stream, the parts that must start at zero (the red-zone bitmap words it uses and the
 //     barrier words), so a call that ended early cannot leave state behind for the next one.
 //     Two calls that overlap on the GPU (different streams without ordering) race on the array:
 //     order them on one stream, or with events.
-//   * Indices >= n are skipped safely (never used as addresses); duplicate indices are the
-//     caller's responsibility, as with rz_remove without RZ_VALIDATE.
+//   * Errors found on the device (an index >= n, a bounded wait that gave up, inconsistent
+//     orphan counts) are ORed into a status word of the array that no call clears; the caller
+//     reads and clears it with rz_noalloc_sync_status, which covers every call since its last use.
+//   * Indices >= n are skipped safely (never used as addresses) and reported as above; duplicate
+//     indices are the caller's responsibility, as with rz_remove without RZ_VALIDATE.
 // The kernel is the grid-wide Redzone body of rz_single_kernel.cuh with its scratch pointers
 // aimed into the array; results are bit-identical to rz_remove.
 #include <algorithm>
@@ -103,8 +108,39 @@ cudaError_t setup_device(int dev, DeviceSetup* out) {
     return cudaSuccess;
 }
 
+// The legacy and per-thread default streams (handles 0, 1, 2) belong to the current device.
+bool stream_on_device(cudaStream_t s, int dev) {
+    if (reinterpret_cast<uintptr_t>(s) <= 2) return true;
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) return false;
+    return sdev == dev;
+}
+
 }  // namespace
 }  // namespace rz
+
+extern "C" int rz_noalloc_sync_status(rz_stream_t stream) {
+    using namespace rz;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RZ_ERR_CUDA;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!stream_on_device(s, dev)) return RZ_ERR_INVALID_ARG;
+    uint32_t* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        base = g_setup[dev].scratch;
+    }
+    if (!base) return cudaStreamSynchronize(s) == cudaSuccess ? RZ_OK : RZ_ERR_CUDA;  // no call on this device yet
+    uint32_t bits = 0;  // pageable host word: the copy completes before the call returns
+    if (cudaMemcpyAsync(&bits, base + kOffStatus, sizeof(bits), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return RZ_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return RZ_ERR_CUDA;
+    if (bits) {
+        if (cudaMemsetAsync(base + kOffStatus, 0, sizeof(uint32_t), s) != cudaSuccess) return RZ_ERR_CUDA;
+        if (cudaStreamSynchronize(s) != cudaSuccess) return RZ_ERR_CUDA;
+    }
+    return map_status(bits);
+}
 
 extern "C" int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_idx, int64_t k,
                                  int64_t* new_len, rz_stream_t stream) {
@@ -121,13 +157,15 @@ extern "C" int rz_remove_noalloc(void* d_data, int64_t n, uint32_t elem_bytes, c
 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RZ_ERR_CUDA;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!stream_on_device(s, dev)) return RZ_ERR_INVALID_ARG;
     DeviceSetup ds;
     if (setup_device(dev, &ds) != cudaSuccess) return RZ_ERR_CUDA;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     uint32_t* base = ds.scratch;
 
-    // Clear what must start at zero: status, epoch, barrier words, and the bitmap words of k bits.
-    if (cudaMemsetAsync(base, 0, kOffBitmap * 4, s) != cudaSuccess) return RZ_ERR_CUDA;
+    // Clear what must start at zero: epoch, barrier words, and the bitmap words of k bits. The
+    // status word is left alone: it collects device errors until rz_noalloc_sync_status reads it.
+    if (cudaMemsetAsync(base + kOffEpoch, 0, (kOffBitmap - kOffEpoch) * 4, s) != cudaSuccess) return RZ_ERR_CUDA;
     if (cudaMemsetAsync(base + kOffBitmap, 0, ((size_t(k) + 31) / 32) * 4, s) != cudaSuccess) return RZ_ERR_CUDA;
 
     NoAllocFn f = noalloc_fn(elem_bytes);
