@@ -42,6 +42,7 @@ NSETS = 8
 SCRUB_BYTES = 256 << 20
 FALLBACK_HBM_GBS = 6650.0
 
+RESULT_BYTES = 520  # one read-back per call: the status word and the device-tracked length
 METRIC = "items removed/s"
 UNIT = "items/s"
 
@@ -259,7 +260,7 @@ def own_arm(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
     import redzone_b200 as rz
-    from redzone_b200 import workloads
+    from redzone_b200 import _native, workloads
     from tests import _torch_rule
 
     ctx = rz.Context(dev.index)
@@ -285,15 +286,15 @@ def own_arm(args):
         return dist.max_over_ranks(x, dev)
 
     # ---- Redzone, device-resident inputs ----
-    for i in range(args.warmup):
-        ctx.remove(a, sets[i % NSETS])
-        scrub.fill_(i & 255)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     clocks = ClockSampler(dev.index)
-    barrier()
     clocks.start()
-    time.sleep(0.25)  # let the sampler attach before the timed region
+    time.sleep(0.25)  # let the sampler attach; the warm-up then runs right before the timed region
+    for i in range(args.warmup):
+        ctx.remove(a, sets[i % NSETS])
+        scrub.fill_(i & 255)
+    barrier()
     region0 = torch.cuda.Event(enable_timing=True)
     region1 = torch.cuda.Event(enable_timing=True)
     region0.record(stream)
@@ -304,8 +305,9 @@ def own_arm(args):
         scrub.fill_(i & 255)
     region1.record(stream)
     barrier()
-    clk = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    step_stats = {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms),
+                  "first": step_ms[: min(8, len(step_ms))]}
     mean_ms = max_over_ranks(statistics.mean(step_ms))
     region_ms = max_over_ranks(region0.elapsed_time(region1))
     value = world * k / (mean_ms * 1e-3)
@@ -349,20 +351,60 @@ def own_arm(args):
     torch.cuda.synchronize()
     part_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in p_ms))
 
-    # ---- end to end through the public C-ABI with host buffers ----
-    e_steps = max(10, min(args.steps, 500))
-    e_ms = []
-    barrier()
-    for i in range(e_steps):
+    # ---- event-timing floor: an empty kernel of the removal's launch shape, timed exactly like a
+    # step (same events, same scrub before it) ----
+    dcfg = ctx.default_cfg(n, k, W_BYTES)
+    cluster = 8 if dcfg.schedule == _native.RZ_SCHED_CSCAN and grid % 8 == 0 else 1
+    f_ev = []
+    for i in range(args.warmup + args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        new_len = ctx.remove_host_idx(a, pinned[i % NSETS])
+        ctx.empty_launch(grid, block, cluster)
         e1.record(stream)
-        assert new_len == n - k
-        e_ms.append((e0, e1))
         scrub.fill_(i & 255)
+        if i >= args.warmup:
+            f_ev.append((e0, e1))
+    torch.cuda.synchronize()
+    floor_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in f_ev))
+
+    # ---- end to end through the public C-ABI with host buffers: every step copies its removal
+    # list from pinned host memory and reads its result (status + device-tracked length) back.
+    # Pipelined: rz_remove_host_idx_async keeps up to E_DEPTH calls in flight, so the copy of
+    # step i+1 overlaps the kernel of step i; each step is collected with rz_wait. No L2 scrub
+    # inside this region (each step's list arrives fresh over PCIe; E_SETS distinct lists) ----
+    E_SETS, E_DEPTH = 64, 4
+    e_np = [workloads.uniform(n, k, seed=dist.replica_seed(1000 + s, rank)) for s in range(E_SETS)]
+    e_pinned = [torch.from_numpy(s.astype(np.int32)).pin_memory() for s in e_np]
+    for i in range(max(args.warmup, E_DEPTH + 1)):  # first use grows the staging slots
+        assert ctx.wait(ctx.remove_host_idx_async(a, e_pinned[i % E_SETS])) == n - k
+    e_steps = max(args.steps, 50)
+    torch.cuda.synchronize()
     barrier()
-    e2e_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in e_ms))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    inflight = []
+    for i in range(e_steps):
+        inflight.append(ctx.remove_host_idx_async(a, e_pinned[i % E_SETS]))
+        if len(inflight) == E_DEPTH:
+            assert ctx.wait(inflight.pop(0)) == n - k
+    for t in inflight:
+        assert ctx.wait(t) == n - k
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e_steps)
+    barrier()
+    clk = clocks.stop()
+    # The synchronous call, one step at a time (copy, kernel, read-back, host wait in series).
+    s_ms = []
+    for i in range(args.warmup + min(e_steps, 200)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        assert ctx.remove_host_idx(a, e_pinned[i % E_SETS]) == n - k
+        e1.record(stream)
+        if i >= args.warmup:
+            s_ms.append((e0, e1))
+    torch.cuda.synchronize()
+    e2e_serial_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in s_ms))
 
     # ---- roofline of the Redzone kernel ----
     balg = statistics.mean(alg_bytes(n, k, W_BYTES, s) for s in sets_np)
@@ -397,8 +439,17 @@ def own_arm(args):
                 "speedup_vs_partition": part_ms / steady_ms,
                 "method": f"CUDA graph of {NSETS} x [removal, 256 MiB scrub] replayed {reps} times, minus the "
                           f"same graph of scrubs alone, divided by the removals"},
+            "step_ms": step_stats,
+            "event_floor_ms": floor_ms,
+            "floor_method": f"empty kernel of the removal's shape ({grid} x {block}, clusters of {cluster}) "
+                            f"between the same events after the same scrub, {args.steps} steps",
+            "removal_share_of_step": max(0.0, (mean_ms - floor_ms) / mean_ms),
             "e2e": {"value": world * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 4 * k,
-                    "d2h_bytes_per_step": 8, "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": RESULT_BYTES, "ms_per_step": e2e_ms, "steps": e_steps,
+                    "method": f"rz_remove_host_idx_async, {E_DEPTH} calls in flight, each step's list copied from "
+                              f"pinned host memory and its status + length read back, rz_wait on every step; "
+                              f"time of the whole region / steps; {E_SETS} distinct lists, no L2 scrub",
+                    "serial_ms_per_step": e2e_serial_ms},
             "cpu_baseline": cpu,
             "clocks": clk,
         }

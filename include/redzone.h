@@ -124,6 +124,25 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
                        rz_stream_t stream);
 
 /*
+ * Pipelined form of rz_remove_host_idx for a host program that hands the GPU one removal list
+ * after another (redzone_CPU, Redzone_CPU.hxx:150, called in a loop): returns without waiting.
+ * The index list is copied on the context's own copy stream, so the copy of one call overlaps
+ * the kernel of the one before; the removal runs on `stream` after its copy, followed by a short
+ * read-back of the call's status and device-tracked length into pinned memory. *ticket names the
+ * call for rz_wait. h_idx (ideally pinned) must stay unchanged until rz_wait for the call returns.
+ * Calls are ordered on `stream` as issued. Up to 4 calls per context are in flight; issuing a 5th
+ * waits for the oldest (its result is kept for rz_wait). The staging buffers grow to the largest
+ * k seen (context scratch). After a device error the status is sticky on the device until the
+ * wait that reads it, so calls issued in between report it too.
+ */
+int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
+                             const uint32_t* h_idx, int64_t k, uint32_t flags, rz_stream_t stream,
+                             uint64_t* ticket);
+/* Wait for the call `ticket` of rz_remove_host_idx_async; returns its status and sets *new_len
+ * (may be NULL) to the length the device tracked. Each ticket is collected once. */
+int rz_wait(rz_ctx* ctx, uint64_t ticket, int64_t* new_len);
+
+/*
  * Add-then-remove (the paper's growth step, Sec. 4.6): append g items from d_gain (device) at
  * rows [n, n + g) of d_data, whose allocation must hold capacity >= n + g items, then remove the k
  * distinct rows d_idx (each < n + g, so appended rows may be removed too) from the grown list with
@@ -426,6 +445,12 @@ int rz_last_launch(const rz_ctx* ctx, int32_t* kernels, int32_t* grid, int32_t* 
  */
 int rz_phase_stamps(rz_ctx* ctx, int enable);
 int rz_read_phase_stamps(rz_ctx* ctx, uint64_t* out, int32_t max_ctas, int32_t* nctas);
+
+/* Measurement aid: launch an empty kernel of `grid` x `block` threads (clusters of `cluster` CTAs,
+ * 1-8, dividing grid; `smem_bytes` of dynamic shared memory) on `stream`. Timed between the same
+ * events as a removal, it gives the floor that every launch of that shape pays. */
+int rz_test_empty_launch(rz_ctx* ctx, int32_t grid, int32_t block, int32_t cluster, int32_t smem_bytes,
+                         rz_stream_t stream);
 
 /*
  * Failure-detection check for the bounded device waits that replace the reference's grid

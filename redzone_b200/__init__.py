@@ -152,6 +152,32 @@ class Context:
         self._check(st, "rz_remove_host_idx")
         return out.value
 
+    def remove_host_idx_async(self, data, h_idx, flags: int = 0, stream=None) -> int:
+        """Pipelined host-index removal (rz_remove_host_idx_async): returns a ticket at once;
+        collect the result with ``wait(ticket)``. ``h_idx`` must stay unchanged until then."""
+        n = int(data.shape[0])
+        if hasattr(h_idx, "data_ptr"):
+            ptr, k = h_idx.data_ptr(), int(h_idx.numel())
+        else:
+            ptr, k = h_idx.ctypes.data, int(h_idx.size)
+        t = ctypes.c_uint64(0)
+        st = _native.lib.rz_remove_host_idx_async(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
+                                                  ctypes.c_void_p(ptr), k, flags,
+                                                  ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(t))
+        self._check(st, "rz_remove_host_idx_async")
+        return t.value
+
+    def wait(self, ticket: int) -> int:
+        """Wait for an rz_remove_host_idx_async call; returns its new length or raises."""
+        out = ctypes.c_int64(0)
+        self._check(_native.lib.rz_wait(self.handle, ctypes.c_uint64(ticket), ctypes.byref(out)), "rz_wait")
+        return out.value
+
+    def empty_launch(self, grid: int, block: int, cluster: int = 1, smem: int = 0, stream=None) -> None:
+        """Launch an empty kernel of the given shape (the event-timing floor of such a launch)."""
+        self._check(_native.lib.rz_test_empty_launch(self.handle, grid, block, cluster, smem,
+                                                     ctypes.c_void_p(_stream_handle(stream))), "rz_test_empty_launch")
+
     def sync_status(self, stream=None) -> int:
         return _native.lib.rz_sync_status(self.handle, ctypes.c_void_p(_stream_handle(stream)))
 

@@ -1,0 +1,216 @@
+// rz_async.cpp -- rz_remove_host_idx_async / rz_wait: the host-index removal, pipelined.
+//
+// rz_remove_host_idx copies the host index list, runs the removal, reads the result back and
+// waits, so consecutive calls run strictly one after another: copy, kernel, read-back, host
+// wake-up. A host program that feeds the GPU a stream of removal lists (the reference's
+// redzone_CPU call shape, Redzone_CPU.hxx:150, called in a loop) can instead issue calls without
+// waiting and collect each result later. Per context there is a ring of kSlots staging slots,
+// each with a device copy of one index list, a pinned copy of the call's status and device
+// length, and two events:
+//   copy stream : H2D  h_idx -> slot.d_idx ; record slot.copied
+//   call stream : wait slot.copied ; removal kernel(s) ; D2H status|length -> slot.h_res ;
+//                 record slot.done
+// The index copy of call i+1 runs on the copy stream while call i's kernel runs, so a caller that
+// keeps a few calls in flight pays for the kernels and the short read-backs, not for the copies.
+// A slot is reused only after its previous call was collected (rz_wait) or, when the caller
+// issues more than kSlots calls ahead, after the issuing call has waited for it and kept its
+// result for a later rz_wait.
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <new>
+
+#include "rz_internal.h"
+
+namespace rz {
+
+namespace {
+
+constexpr int kSlots = 4;
+constexpr size_t kStashMax = 1024;  // results of calls evicted from their slot before rz_wait
+
+struct Slot {
+    uint32_t* d_idx = nullptr;
+    size_t cap = 0;                  // entries of d_idx
+    uint8_t* h_res = nullptr;        // pinned: status word at 0, device length at 512
+    cudaEvent_t copied = nullptr;
+    cudaEvent_t done = nullptr;
+    uint64_t ticket = 0;
+    int64_t k = 0, n = 0;
+    bool pending = false;
+};
+
+struct Result {
+    uint64_t ticket;
+    int status;
+    int64_t new_len;
+};
+
+}  // namespace
+
+struct AsyncPipe {
+    cudaStream_t copy_stream = nullptr;
+    Slot slots[kSlots];
+    std::deque<Result> stash;
+    uint64_t next_ticket = 1;
+};
+
+namespace {
+
+int pipe_create(rz_ctx* ctx, AsyncPipe** out) {
+    AsyncPipe* p = new (std::nothrow) AsyncPipe();
+    if (!p) return RZ_ERR_NO_MEMORY;
+    cudaError_t e = cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking);
+    for (int i = 0; i < kSlots && e == cudaSuccess; ++i) {
+        Slot& s = p->slots[i];
+        void* h = nullptr;
+        e = cudaMallocHost(&h, kResultBytes);
+        if (e != cudaSuccess) break;
+        s.h_res = static_cast<uint8_t*>(h);
+        e = cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        const int st = cuda_fail(ctx, e, "asynchronous pipeline");
+        for (Slot& s : p->slots) {
+            if (s.h_res) cudaFreeHost(s.h_res);
+            if (s.copied) cudaEventDestroy(s.copied);
+            if (s.done) cudaEventDestroy(s.done);
+        }
+        if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+        delete p;
+        return st;
+    }
+    *out = p;
+    return RZ_OK;
+}
+
+// The finished call of a pending slot: its status (mapped) and device-tracked length. A device
+// error marks the context scratch for a reset before its next call and clears the status word.
+int collect(rz_ctx* ctx, Slot& s, Result* r) {
+    const int st = wait_event(ctx, s.done);
+    if (st != RZ_OK) return st;
+    uint32_t bits = 0;
+    unsigned long long len = 0;
+    std::memcpy(&bits, s.h_res, sizeof(bits));
+    std::memcpy(&len, s.h_res + 512, sizeof(len));
+    s.pending = false;
+    if (bits) {
+        RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
+        ctx->ws.dirty = true;
+    }
+    r->ticket = s.ticket;
+    r->status = map_status(bits);
+    r->new_len = (s.k > 0 && s.k < s.n) ? int64_t(len) : s.n - s.k;
+    return RZ_OK;
+}
+
+}  // namespace
+
+void release_async(rz_ctx* ctx) {
+    AsyncPipe* p = static_cast<AsyncPipe*>(ctx->async_pipe);
+    if (!p) return;
+    cudaStreamSynchronize(p->copy_stream);
+    for (Slot& s : p->slots) {
+        if (s.done) cudaEventSynchronize(s.done);
+        cudaFree(s.d_idx);
+        if (s.h_res) cudaFreeHost(s.h_res);
+        if (s.copied) cudaEventDestroy(s.copied);
+        if (s.done) cudaEventDestroy(s.done);
+    }
+    cudaStreamDestroy(p->copy_stream);
+    delete p;
+    ctx->async_pipe = nullptr;
+}
+
+}  // namespace rz
+
+using namespace rz;
+
+extern "C" {
+
+int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* h_idx,
+                             int64_t k, uint32_t flags, rz_stream_t stream, uint64_t* ticket) {
+    if (!ctx || !ticket) return RZ_ERR_INVALID_ARG;
+    *ticket = 0;
+    if (n < 0 || k < 0 || k > n || (k > 0 && (!d_data || !h_idx))) return RZ_ERR_INVALID_ARG;
+    if (n >= (int64_t(1) << 32)) return RZ_ERR_UNSUPPORTED;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!ctx->async_pipe) {
+        AsyncPipe* p = nullptr;
+        const int st = pipe_create(ctx, &p);
+        if (st != RZ_OK) return st;
+        ctx->async_pipe = p;
+    }
+    AsyncPipe& P = *static_cast<AsyncPipe*>(ctx->async_pipe);
+    const uint64_t t = P.next_ticket;
+    Slot& s = P.slots[t % kSlots];
+    if (s.pending) {
+        // The caller is more than kSlots calls ahead: finish the slot's call and keep its result.
+        Result r;
+        const int st = collect(ctx, s, &r);
+        if (st != RZ_OK) return st;
+        P.stash.push_back(r);
+        if (P.stash.size() > kStashMax) P.stash.pop_front();
+    }
+    if (size_t(k) + 1 > s.cap) {
+        // Grow the slot's staging (its previous call, if any, has finished).
+        const size_t want = std::max<size_t>(size_t(k) + 1, 2 * s.cap);
+        if (s.d_idx) {
+            RZ_CUDA_TRY(ctx, cudaFree(s.d_idx));
+            ctx->scratch_held -= s.cap * 4;
+            s.d_idx = nullptr;
+            s.cap = 0;
+        }
+        if (ctx->scratch_held + want * 4 > ctx->scratch_limit) {
+            ctx->last_cuda_error = "context scratch limit reached";
+            return RZ_ERR_NO_MEMORY;
+        }
+        void* d = nullptr;
+        RZ_CUDA_TRY(ctx, cudaMalloc(&d, want * 4));
+        s.d_idx = static_cast<uint32_t*>(d);
+        s.cap = want;
+        ctx->scratch_held += want * 4;
+    }
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    if (k > 0) {
+        RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.d_idx, h_idx, size_t(k) * 4, cudaMemcpyHostToDevice, P.copy_stream));
+        RZ_CUDA_TRY(ctx, cudaEventRecord(s.copied, P.copy_stream));
+        RZ_CUDA_TRY(ctx, cudaStreamWaitEvent(cs, s.copied, 0));
+    }
+    const int st = rz_remove(ctx, d_data, n, elem_bytes, s.d_idx, k, nullptr, flags & ~uint32_t(RZ_SYNC), stream);
+    if (st != RZ_OK) return st;
+    RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.h_res, ctx->ws.status, kResultBytes, cudaMemcpyDeviceToHost, cs));
+    RZ_CUDA_TRY(ctx, cudaEventRecord(s.done, cs));
+    s.ticket = t;
+    s.k = k;
+    s.n = n;
+    s.pending = true;
+    P.next_ticket = t + 1;
+    *ticket = t;
+    return RZ_OK;
+}
+
+int rz_wait(rz_ctx* ctx, uint64_t ticket, int64_t* new_len) {
+    if (!ctx || ticket == 0) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    AsyncPipe* p = static_cast<AsyncPipe*>(ctx->async_pipe);
+    if (!p || ticket >= p->next_ticket) return RZ_ERR_INVALID_ARG;
+    Slot& s = p->slots[ticket % kSlots];
+    Result r{};
+    if (s.pending && s.ticket == ticket) {
+        const int st = collect(ctx, s, &r);
+        if (st != RZ_OK) return st;
+    } else {
+        auto it = std::find_if(p->stash.begin(), p->stash.end(), [&](const Result& x) { return x.ticket == ticket; });
+        if (it == p->stash.end()) return RZ_ERR_INVALID_ARG;  // already collected, or too old
+        r = *it;
+        p->stash.erase(it);
+    }
+    if (new_len) *new_len = r.new_len;
+    return r.status;
+}
+
+}  // extern "C"

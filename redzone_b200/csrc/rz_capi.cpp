@@ -106,10 +106,9 @@ int map_status(uint32_t bits) {
 // in one copy on the call's stream into pinned memory. The caller waits for it by polling an
 // event recorded after the copy, so a synchronous call returns within about a microsecond of
 // the copy landing; after kPollLimit of polling it blocks in cudaEventSynchronize instead.
-static constexpr size_t kResultBytes = 512 + sizeof(unsigned long long);
 static constexpr std::chrono::microseconds kPollLimit{2000};
 
-static int wait_event(rz_ctx* ctx, cudaEvent_t ev) {
+int wait_event(rz_ctx* ctx, cudaEvent_t ev) {
     const auto t0 = std::chrono::steady_clock::now();
     bool polled = false;
     for (;;) {
@@ -460,6 +459,14 @@ int rz_read_phase_stamps(rz_ctx* ctx, uint64_t* out, int32_t max_ctas, int32_t* 
         RZ_CUDA_TRY(ctx, cudaMemcpy(out, ctx->ws.stamps, size_t(n) * kStampsPerCta * 8, cudaMemcpyDeviceToHost));
     if (nctas) *nctas = n;
     return RZ_OK;
+}
+
+int rz_test_empty_launch(rz_ctx* ctx, int32_t grid, int32_t block, int32_t cluster, int32_t smem_bytes,
+                         rz_stream_t stream) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return test_empty_launch(ctx, grid, block, cluster, smem_bytes, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int rz_test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_bits) {

@@ -69,6 +69,7 @@ struct rz_ctx {
     int last_block = 0;
     void* predictor = nullptr;   // rz::Predictor*, owned (see rz_mlp.cu)
     void* tune_table = nullptr;  // rz::TuneTable*, owned (see rz_autotune.cpp)
+    void* async_pipe = nullptr;  // rz::AsyncPipe*, owned (see rz_async.cpp)
     size_t scratch_held = 0;     // bytes of grown context scratch
     size_t scratch_limit = ~size_t(0);  // rz_set_scratch_limit: growth beyond it -> RZ_ERR_NO_MEMORY
     cudaEvent_t done_event = nullptr;    // completion of a synchronous call's last copy (polled)
@@ -146,6 +147,11 @@ bool predict_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, const uint32_t
                  cudaStream_t s, rz_launch_cfg* cfg);
 bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
 void release_extras(rz_ctx* ctx);
+// The status word (offset 0) and the device length (offset 512) of the workspace block: one
+// device-to-host copy of this many bytes brings both back.
+constexpr size_t kResultBytes = 512 + sizeof(unsigned long long);
+// Wait for an event: poll (about 2 ms), then block. RZ_OK or RZ_ERR_CUDA.
+int wait_event(rz_ctx* ctx, cudaEvent_t ev);
 // Map device status bits (ST_* of rz_common.cuh) to an rz_status code, most severe first.
 int map_status(uint32_t bits);
 // Wait for the stream, then map the device status to rz_status (clearing it); with new_len, also
@@ -161,5 +167,7 @@ int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStrea
 // Test hook: run a grid barrier whose expected arrival count exceeds the grid, so that the
 // bounded wait must expire; returns the device status bits observed.
 int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out);
+// Diagnostic: launch an empty kernel of the given shape (cluster size 1-8 dividing grid).
+int test_empty_launch(rz_ctx* ctx, int grid, int block, int cluster, int smem, cudaStream_t s);
 
 }  // namespace rz

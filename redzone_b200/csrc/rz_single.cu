@@ -331,6 +331,30 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     return RZ_OK;
 }
 
+// An empty kernel: what a launch of a given shape costs between two events with no work in it.
+__global__ void empty_launch_kernel() {}
+
+int test_empty_launch(rz_ctx* ctx, int grid, int block, int cluster, int smem, cudaStream_t s) {
+    if (grid < 1 || block < 1 || block > 1024 || cluster < 1 || cluster > 8 || grid % cluster || smem < 0)
+        return RZ_ERR_INVALID_ARG;
+    if (smem > 48 * 1024)
+        RZ_CUDA_TRY(ctx, cudaFuncSetAttribute(empty_launch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(unsigned(grid));
+    lc.blockDim = dim3(unsigned(block));
+    lc.dynamicSmemBytes = size_t(smem);
+    lc.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = unsigned(cluster);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = cluster > 1 ? 1 : 0;
+    RZ_CUDA_TRY(ctx, cudaLaunchKernelEx(&lc, empty_launch_kernel));
+    return RZ_OK;
+}
+
 int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out) {
     cudaStream_t s = nullptr;
     int st = reset_if_dirty(ctx, s);

@@ -1,0 +1,98 @@
+"""rz_remove_host_idx_async / rz_wait: the pipelined host-index removal, against the oracle.
+
+Calls are issued back to back on one list (each removes from what the previous one left, as a
+host program feeding removal lists in a loop would), with more calls in flight than the context
+has staging slots, with growing k, and with every item width; each result is checked against
+the oracle applied in the same order."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import redzone_b200 as rz
+from redzone_b200 import _native, workloads
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = rz.Context(0)
+    yield c
+    c.close()
+
+
+def _chain(n0, ks, seed):
+    """Index lists of a chain of removals: list j removes ks[j] items from the length left."""
+    out, n = [], n0
+    for j, k in enumerate(ks):
+        dist = ("uniform", "red30", "clustered", "tail")[j % 4]
+        if dist == "clustered" and k < 256:
+            dist = "uniform"
+        out.append(workloads.make(dist, n, k, seed + j))
+        n -= k
+    return out
+
+
+@pytest.mark.parametrize("words", [1, 2, 4, 8])
+def test_async_chain_matches_oracle(ctx, words):
+    n0 = 1 << 20
+    ks = [1000, 1 << 14, 5, 1 << 16, 300, 1 << 12, 70000, 1 << 10, 2, 1 << 15]
+    lists = _chain(n0, ks, seed=40 + words)
+    rng = np.random.default_rng(words)
+    host = rng.integers(0, 1 << 32, size=(n0, words), dtype=np.uint64).astype(np.uint32)
+    d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+    pinned = [torch.from_numpy(x.astype(np.int32)).pin_memory() for x in lists]
+    # Issue every call before collecting any (10 calls > the context's 4 slots).
+    n, tickets = n0, []
+    for x in pinned:
+        tickets.append(ctx.remove_host_idx_async(d[:n], x))
+        n -= x.numel()
+    exp = host.copy()
+    n = n0
+    for t, x in zip(tickets, lists):
+        assert ctx.wait(t) == n - x.size
+        sub = exp[:n].copy()
+        oracle.remove(sub, x)
+        exp[:n - x.size] = sub[:n - x.size]
+        n -= x.size
+    got = d.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got[:n], exp[:n])
+
+
+def test_async_interleaved_waits_and_errors(ctx):
+    n = 1 << 18
+    a = torch.arange(n, dtype=torch.int32, device=DEV)
+    b = a.clone()
+    idx = [workloads.uniform(n, 4096, seed=s).astype(np.int32) for s in range(6)]
+    pinned = [torch.from_numpy(x).pin_memory() for x in idx]
+    # Each call removes from the full length n of its own array copy: results are independent.
+    arrays = [a.clone() for _ in idx]
+    tickets = [ctx.remove_host_idx_async(arr, x) for arr, x in zip(arrays, pinned)]
+    # Collect out of order.
+    for j in (3, 0, 5, 1, 4, 2):
+        assert ctx.wait(tickets[j]) == n - 4096
+    for arr, x in zip(arrays, idx):
+        exp = np.arange(n, dtype=np.int32)
+        oracle.remove(exp, x.astype(np.uint32))
+        assert np.array_equal(arr[: n - 4096].cpu().numpy(), exp[: n - 4096])
+    # A ticket is collected once.
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.wait(tickets[0])
+    assert e.value.code == _native.RZ_ERR_INVALID_ARG
+    # A duplicate under RZ_VALIDATE comes back from rz_wait, with the list untouched.
+    bad = idx[0].copy()
+    bad[10] = bad[11]
+    pb = torch.from_numpy(bad).pin_memory()
+    t = ctx.remove_host_idx_async(b, pb, flags=rz.RZ_VALIDATE)
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.wait(t)
+    assert e.value.code == _native.RZ_ERR_DUPLICATE
+    assert torch.equal(b, torch.arange(n, dtype=torch.int32, device=DEV))
+    # The context is usable afterwards.
+    t = ctx.remove_host_idx_async(b, pinned[1])
+    assert ctx.wait(t) == n - 4096
+    exp = np.arange(n, dtype=np.int32)
+    oracle.remove(exp, idx[1].astype(np.uint32))
+    assert np.array_equal(b[: n - 4096].cpu().numpy(), exp[: n - 4096])
