@@ -412,6 +412,13 @@ def own_arm(args):
     peak, peak_kind = load_peaks()
     traffic = load_traffic(f"redzone_single_n2e{N_LOG2}_k2e{K_LOG2}_w{W_BYTES}")
 
+    # ---- the batched half of the metric: 4096 uneven lists in one launch against per-list launches ----
+    bat = None
+    if not args.no_batched:
+        del a, sets, scrub
+        torch.cuda.empty_cache()
+        bat = batched_leg(args, ctx, dev, world, rank, steps=max(5, min(args.steps, 20)), warmup=args.warmup)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         kind, cores, times, rz_cpu, par, host = cpu_baselines(n, k, 50, 2, 20.0, par_calls=3)
@@ -451,6 +458,7 @@ def own_arm(args):
                               f"time of the whole region / steps; {E_SETS} distinct lists, no L2 scrub",
                     "serial_ms_per_step": e2e_serial_ms},
             "cpu_baseline": cpu,
+            "batched": bat,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -511,26 +519,13 @@ def sweep(args):
         torch.cuda.empty_cache()
 
 
-def batched(args):
-    """4096 uneven lists (n log-uniform in [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), uint64
-    payload = list id << 32 | index): one persistent graph-replayed launch against one rz_remove
-    launch per list (stream-launched, and the same launches captured in one CUDA graph)."""
+def make_batched_lists(args, dev, world, rank):
+    """This rank's share of the batched workload on the device: (lists, n, k of all lists)."""
     import torch
-    import redzone_b200 as rz
-    from redzone_b200 import _native, dist, workloads
+    from redzone_b200 import dist, workloads
 
-    # N > 1: the lists are partitioned across ranks by removals (contiguous, balanced), each rank
-    # runs its share as one launch; no collective on the data path, max-over-ranks timing.
-    world, rank, local = dist.init("nccl")
-    if world == 1:
-        torch.cuda.set_device(0)
-    dev = torch.device("cuda", torch.cuda.current_device())
-    ctx = rz.Context(dev.index)
-    nlists_all = args.lists
-    n_all, k_all = workloads.batched_lists(nlists_all, seed=args.seed)
-    total_n, total_k = int(n_all.sum()), int(k_all.sum())
+    n_all, k_all = workloads.batched_lists(args.lists, seed=args.seed)
     mine = dist.shard_by_weight(k_all, world, rank)
-    nlists = len(mine)
     n, k = n_all[mine], k_all[mine]
     buf = torch.empty(int(n.sum()), dtype=torch.int64, device=dev)
     g = torch.Generator(device=dev)
@@ -544,9 +539,24 @@ def batched(args):
         idx = torch.randperm(ni, generator=g, device=dev)[:ki].to(torch.int32)
         lists.append((seg, idx))
         off += ni
-    stream = torch.cuda.current_stream()
+    return lists, n_all, k_all
 
+
+def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) -> dict:
+    """4096 uneven lists (n log-uniform in [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), uint64
+    payload = list id << 32 | index): one persistent graph-replayed launch against one rz_remove
+    launch per list (stream-launched, and the same launches captured in one CUDA graph). N > 1:
+    the lists are partitioned across ranks by removals (contiguous, balanced), each rank runs its
+    share as one launch; no collective on the data path, max-over-ranks timing."""
+    import torch
+    import redzone_b200 as rz
+    from redzone_b200 import _native, dist
     from tests import _torch_rule
+
+    lists, n_all, k_all = make_batched_lists(args, dev, world, rank)
+    nlists = len(lists)
+    total_n, total_k = int(n_all.sum()), int(k_all.sum())
+    stream = torch.cuda.current_stream()
     tuned = _native.BatchCfg()
     best_ms = _native.c_f32(0)
     cfg = None
@@ -568,6 +578,7 @@ def batched(args):
     for l in sample:
         ni, ki = lists[l][0].shape[0], lists[l][1].numel()
         assert torch.equal(lists[l][0][: ni - ki], exp[l]), f"batched parity failed on list {l}"
+    del exp
 
     def timed(fn, reps):
         ts = []
@@ -580,51 +591,78 @@ def batched(args):
             ts.append(e0.elapsed_time(e1))
         return statistics.median(ts)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plan.launch()
     dist.barrier(dev)
-    batched_ms = dist.max_over_ranks(timed(plan.launch, args.steps), dev)
+    batched_ms = dist.max_over_ranks(timed(plan.launch, steps), dev)
 
     def plain():
         for d, i in lists:
             ctx.remove(d, i)
     plain()
-    plain_ms = dist.max_over_ranks(timed(plain, max(3, args.steps // 5)), dev)
+    plain_ms = dist.max_over_ranks(timed(plain, max(3, steps // 5)), dev)
     # The same per-list launches captured once into a CUDA graph (no host launch overhead).
     plain_graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(plain_graph):
         plain()
     plain_graph.replay()
-    plain_graph_ms = dist.max_over_ranks(timed(plain_graph.replay, max(3, args.steps // 5)), dev)
+    plain_graph_ms = dist.max_over_ranks(timed(plain_graph.replay, max(3, steps // 5)), dev)
     del plain_graph
     info = plan.info()
+    plan.close()
     w = 8
     # Algorithmic bytes: red-zone entries estimated from a sample of this rank's lists.
     kr_s = k_s = 0
     for d, i in lists[:: max(1, nlists // 256)]:
         kr_s += int((i >= d.shape[0] - i.numel()).sum().item())
         k_s += i.numel()
-    k_r = total_k * (kr_s / max(1, k_s))
-    balg = 4.0 * total_k + 2.0 * w * (total_k - k_r) + total_k / 4.0
+    my_k = sum(i.numel() for _, i in lists)
+    k_r = my_k * (kr_s / max(1, k_s))
+    balg = 4.0 * my_k + 2.0 * w * (my_k - k_r) + my_k / 4.0
     peak, peak_kind = load_peaks()
-    line = {
-        "metric": METRIC, "value": total_k / (batched_ms * 1e-3), "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"{nlists_all} lists, n log-uniform [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), "
-                               f"uint64 payload (list id << 32 | index), one persistent graph-replayed launch per GPU",
-                   "total_n": total_n, "total_k": total_k, "batch_cfg": info,
-                   "parallelism": "single GPU" if world == 1 else f"{world} GPUs, lists partitioned by removals",
-                   "tuned_ms": float(best_ms.value) if cfg is not None else None},
+    del lists
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"{args.lists} lists, n log-uniform [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), "
+                    f"uint64 payload (list id << 32 | index), one persistent graph-replayed launch per GPU",
+        "total_n": total_n, "total_k": total_k, "batch_cfg": info,
+        "tuned_ms": float(best_ms.value) if cfg is not None else None,
+        "items_per_s": total_k / (batched_ms * 1e-3), "ms_per_launch": batched_ms, "steps": steps,
+        "parallelism": "single GPU" if world == 1 else f"{world} GPUs, lists partitioned by removals",
         "plain_per_list": {"ms_per_step": plain_ms, "speedup_batched_vs_plain": plain_ms / batched_ms},
-        "plain_per_list_graph": {"ms_per_step": plain_graph_ms, "speedup_batched_vs_plain": plain_graph_ms / batched_ms},
+        "plain_per_list_graph": {"ms_per_step": plain_graph_ms,
+                                 "speedup_batched_vs_plain": plain_graph_ms / batched_ms},
+        "speedup_vs_plain": plain_ms / batched_ms,
         "roofline": {"bound": "hbm", "achieved": balg / (batched_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": balg / (batched_ms * 1e-3) / 1e9 / peak, "traffic": None, "alg_bytes_per_launch": balg},
-        "gpu_launches": args.steps,
+                     "frac": balg / (batched_ms * 1e-3) / 1e9 / peak, "traffic": None,
+                     "alg_bytes_per_launch": balg, "peak_source": peak_kind},
+        "parity": f"{len(sample)} sampled lists bit-exact against the canonical rule before timing",
+    }
+
+
+def batched(args):
+    """--workload batched: the batched leg as its own JSON line."""
+    import torch
+    import redzone_b200 as rz
+    from redzone_b200 import dist
+
+    world, rank, local = dist.init("nccl")
+    if world == 1:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ctx = rz.Context(dev.index)
+    b = batched_leg(args, ctx, dev, world, rank, args.steps, args.warmup)
+    line = {
+        "metric": METRIC, "value": b["items_per_s"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": b["ms_per_launch"], "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": b["workload"], "total_n": b["total_n"], "total_k": b["total_k"],
+                   "batch_cfg": b["batch_cfg"], "parallelism": b["parallelism"], "tuned_ms": b["tuned_ms"]},
+        "plain_per_list": b["plain_per_list"], "plain_per_list_graph": b["plain_per_list_graph"],
+        "roofline": b["roofline"], "gpu_launches": args.steps,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    plan.close()
     ctx.close()
     if world > 1:
         import torch.distributed as tdist
@@ -828,6 +866,7 @@ def main():
     ap.add_argument("--lists", type=int, default=4096, help="--workload batched: number of lists")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true", help="--workload batched: skip the autotuner")
+    ap.add_argument("--no-batched", action="store_true", help="default run: skip the batched leg")
     ap.add_argument("--config", default=None,
                     help="JSON file of option defaults, e.g. {\"workload\": \"service\", \"rate\": 40000}; "
                          "flags on the command line override it")

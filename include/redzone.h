@@ -290,13 +290,18 @@ typedef struct rz_batch_cfg {
     int32_t items;
     int32_t ctas_per_sm;
     int32_t span;
+    int32_t wave;  /* work order: 0 = phase by phase over all lists (every list's marks, then the    */
+                   /* holes of every list, then every list's orphans); w > 0 = list by list, a     */
+                   /* list's phases w/2 grids' worth of work items apart (keeps its writes in L2) */
 } rz_batch_cfg;
 
 typedef struct rz_batch_plan rz_batch_plan;
 
 /*
  * Plan the removal of every list of `lists` (host array) in one persistent launch. The plan owns
- * its work queue and scratch. cfg == NULL uses the context's tuned batched configuration.
+ * its work queue and scratch. cfg == NULL uses the configuration the list-mix predictor picks
+ * when one is attached (rz_set_batch_predictor), else the context's tuned batched configuration,
+ * else the built-in default.
  * Each list's result equals rz_remove on that list (the reference's per-list calls,
  * redzone.hxx:1089-1166, one launch each).
  */
@@ -390,7 +395,7 @@ int rz_autotune_batched(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, 
                         int32_t reps, rz_batch_cfg* best, float* best_ms);
 /*
  * Tuning tables (text; '#' comments; lines "single <w> <log2k> <block> <items> <g> <partition>
- * [<schedule>]" and "batched <w> <block> <items> <ctas_per_sm>"). rz_remove and rz_batch_plan_create use the
+ * [<schedule>]" and "batched <w> <block> <items> <ctas_per_sm> [<wave>]"). rz_remove and rz_batch_plan_create use the
  * loaded entries (nearest log2 k bucket of the same width).
  */
 int rz_tune_table_load(rz_ctx* ctx, const char* path);
@@ -430,6 +435,22 @@ int  rz_set_predictor(rz_ctx* ctx, rz_mlp* mlp);
 /* The configuration the attached predictor picks for an instance. */
 int  rz_predict_cfg(rz_ctx* ctx, const uint32_t* d_idx, int64_t n, int64_t k, uint32_t elem_bytes,
                     rz_launch_cfg* cfg);
+/*
+ * The same network trained for mixes of lists: it picks the batched kernel's configuration
+ * (block {128,256,512} x items {2,4,8} x CTAs per SM {1,2,4} x work order {0, 6}: the 54 points
+ * of rz_batch_config_space, in that order = outputs 0..53; the other outputs are ignored; the
+ * autotuner searches the same space) from 12 features of the mix that rz_batch_features
+ * computes on the host from the list sizes: log2 of the list count, total n and total k, total
+ * k / n, payload bytes, mean and spread of log2 n, mean k/n, the share of removals in lists with
+ * k <= 256 / 1024 / 4096, log2 of the largest k. No counterpart in the reference (it has no
+ * batching). rz_set_batch_predictor attaches it (NULL detaches): rz_batch_plan_create and
+ * rz_remove_batched then use its choice; rz_predict_batch_cfg returns it.
+ */
+int  rz_batch_config_space(rz_batch_cfg* out, int32_t max);
+int  rz_batch_features(const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes, float* h_features12);
+int  rz_set_batch_predictor(rz_ctx* ctx, rz_mlp* mlp);
+int  rz_predict_batch_cfg(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
+                          rz_batch_cfg* cfg);
 
 /* ---- diagnostics -------------------------------------------------------------------------- */
 /* Number of kernels the context's most recent removal call launched (memsets not counted), and

@@ -58,10 +58,14 @@ class ListDesc(ctypes.Structure):
 
 
 class BatchCfg(ctypes.Structure):
-    _fields_ = [("block", c_i32), ("items", c_i32), ("ctas_per_sm", c_i32), ("span", c_i32)]
+    _fields_ = [("block", c_i32), ("items", c_i32), ("ctas_per_sm", c_i32), ("span", c_i32), ("wave", c_i32)]
+
+    def as_tuple(self):
+        return (self.block, self.items, self.ctas_per_sm, self.span, self.wave)
 
     def __repr__(self):
-        return f"BatchCfg(block={self.block}, items={self.items}, ctas_per_sm={self.ctas_per_sm})"
+        return (f"BatchCfg(block={self.block}, items={self.items}, ctas_per_sm={self.ctas_per_sm}, "
+                f"span={self.span}, wave={self.wave})")
 
 
 class TuneEntry(ctypes.Structure):
@@ -174,6 +178,10 @@ _sig("rz_mlp_gradients", c_i32, [c_vp, _FP, _FP, c_i64, _FP, _FP])
 _sig("rz_mlp_train", c_i32, [c_vp, _FP, _FP, c_i64, c_i32, c_i32, c_f32, c_u64, _FP])
 _sig("rz_set_predictor", c_i32, [c_vp, c_vp])
 _sig("rz_predict_cfg", c_i32, [c_vp, c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchCfg)])
+_sig("rz_batch_config_space", c_i32, [ctypes.POINTER(BatchCfg), c_i32])
+_sig("rz_batch_features", c_i32, [ctypes.POINTER(ListDesc), c_i32, c_u32, _FP])
+_sig("rz_set_batch_predictor", c_i32, [c_vp, c_vp])
+_sig("rz_predict_batch_cfg", c_i32, [c_vp, ctypes.POINTER(ListDesc), c_i32, c_u32, ctypes.POINTER(BatchCfg)])
 _sig("rz_phase_stamps", c_i32, [c_vp, c_i32])
 _sig("rz_read_phase_stamps", c_i32, [c_vp, ctypes.POINTER(c_u64), c_i32, ctypes.POINTER(c_i32)])
 

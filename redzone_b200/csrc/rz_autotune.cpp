@@ -65,6 +65,7 @@ bool default_batch_cfg(const rz_ctx* ctx, uint32_t w, rz_batch_cfg* cfg) {
     cfg->items = 8;
     cfg->ctas_per_sm = 4;
     cfg->span = 0;
+    cfg->wave = kDefaultWave;
     if (w >= 16) cfg->items = 4;
     if (ctx->tune_table) {
         TuneTable* t = static_cast<TuneTable*>(ctx->tune_table);
@@ -180,10 +181,8 @@ int rz_autotune_batched(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, 
     int st = ensure_scrub(ctx);
     if (st != RZ_OK) return st;
     TuneTable* t = table(ctx);
-    std::vector<rz_batch_cfg> cands;
-    for (int b : {128, 256, 512})
-        for (int i : {2, 4, 8})
-            for (int c : {1, 2, 4, 8}) cands.push_back(rz_batch_cfg{b, i, c, 0});
+    std::vector<rz_batch_cfg> cands(kBatchCfgSpace);
+    batch_config_space(cands.data());
     cudaStream_t s = nullptr;
     RZ_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     cudaEvent_t e0, e1;
@@ -250,7 +249,8 @@ int rz_tune_table_save(rz_ctx* ctx, const char* path) {
         std::fprintf(f, "single %u %d %d %d %d %d %d\n", kv.first.first, kv.first.second, kv.second.block,
                      kv.second.items, kv.second.ctas_per_sm, kv.second.use_partition, kv.second.schedule);
     for (auto& kv : t->batched)
-        std::fprintf(f, "batched %u %d %d %d\n", kv.first, kv.second.block, kv.second.items, kv.second.ctas_per_sm);
+        std::fprintf(f, "batched %u %d %d %d %d\n", kv.first, kv.second.block, kv.second.items, kv.second.ctas_per_sm,
+                     kv.second.wave);
     std::fclose(f);
     return RZ_OK;
 }
@@ -277,11 +277,12 @@ int rz_tune_table_load(rz_ctx* ctx, const char* path) {
             }
             t->single[{w, a}] = rz_launch_cfg{b, c, d, e, got >= 7 ? sc : RZ_SCHED_AUTO};
         } else if (std::strcmp(kind, "batched") == 0) {
-            if (std::sscanf(line, "%*s %u %d %d %d", &w, &a, &b, &c) != 4) {
+            int wave = 0;  // optional fifth number (older tables have four)
+            if (std::sscanf(line, "%*s %u %d %d %d %d", &w, &a, &b, &c, &wave) < 4) {
                 ++bad;
                 continue;
             }
-            t->batched[w] = rz_batch_cfg{a, b, c, 0};
+            t->batched[w] = rz_batch_cfg{a, b, c, 0, wave};
         } else {
             ++bad;
         }

@@ -12,9 +12,11 @@
 //                  orphans of its tiles by global rank (the grid kernel's phase C)
 // A waiting item only ever waits for items with smaller tickets, which running CTAs took and finish
 // without waiting on anything later, so the queue cannot deadlock; every wait is bounded anyway.
-// SINGLE items sit between the MARK and CLASSIFY blocks so that the marks have landed by the time
-// the first CLASSIFY item is taken. Reference: the per-block body of Algorithm 1
-// (RemoveFromList2, redzone.hxx:237-444) and the phases of Algorithm 2 (redzone.hxx:626-941).
+// The queue runs phase by phase over all lists (SINGLE items between the MARK and CLASSIFY items,
+// so that the marks have landed by the time the first CLASSIFY item is taken), or, with
+// rz_batch_cfg.wave > 0, as a wavefront over the lists (order_queue). Reference: the per-block
+// body of Algorithm 1 (RemoveFromList2, redzone.hxx:237-444) and the phases of Algorithm 2
+// (redzone.hxx:626-941).
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -375,6 +377,66 @@ static uint32_t span_for(uint32_t nch, int32_t cfg_span) {
     return std::max<uint32_t>(1u, std::min<uint32_t>(8u, nch / 32u));
 }
 
+// Queue order. With lag == 0, phase by phase over all lists. Otherwise the multi-tile lists run
+// as a wavefront, list after list: a list's CLASSIFY items follow its MARK items, and its PAIR
+// items its CLASSIFY items, by about `lag` tickets (a grid or more, so what an item waits for was
+// taken a full round of the grid earlier and has normally finished). A list's phases thus run close together in time: the index list is
+// read again while still in L2, and its hole writes -- classified and orphan ones alike -- land
+// while the lines of its prefix are still in L2, where writes to the same 32-byte sector merge
+// before one write-back. MARK items run ahead of the wavefront by at most 2 lag; SINGLE items fill
+// the gaps the lags leave. Every item still follows everything it waits for (MARK before
+// CLASSIFY before PAIR of the same list), so no wait can deadlock.
+// mark / classify / pair hold the groups of each multi-tile list in list order; `groups` holds
+// each such list's group count, in the same order.
+static void order_queue(const std::vector<uint2>& mark, const std::vector<uint2>& single,
+                        const std::vector<uint2>& classify, const std::vector<uint2>& pair,
+                        const std::vector<uint32_t>& groups, size_t lag, std::vector<uint2>& out) {
+    out.clear();
+    if (lag == 0) {
+        // Phase by phase: every MARK item, the SINGLE items (largest first, while the marks land),
+        // every CLASSIFY item, every PAIR item.
+        out.reserve(mark.size() + single.size() + classify.size() + pair.size());
+        out.insert(out.end(), mark.begin(), mark.end());
+        out.insert(out.end(), single.begin(), single.end());
+        out.insert(out.end(), classify.begin(), classify.end());
+        out.insert(out.end(), pair.begin(), pair.end());
+        return;
+    }
+    const size_t nb = groups.size();
+    std::vector<size_t> first(nb + 1, 0);  // first item of block b in mark / classify / pair
+    for (size_t b = 0; b < nb; ++b) first[b + 1] = first[b] + groups[b];
+    std::vector<size_t> last_m(nb, 0), last_c(nb, 0);
+    size_t im = 0, ic = 0, ip = 0, is = 0;  // items emitted from each stream
+    size_t bm = 0, bc = 0, bp = 0;          // block of the next item of each stream
+    const size_t total = mark.size() + single.size() + classify.size() + pair.size();
+    out.clear();
+    out.reserve(total);
+    auto pos = [&]() { return out.size(); };
+    auto emit_m = [&]() {
+        out.push_back(mark[im++]);
+        if (im == first[bm + 1]) last_m[bm++] = pos();
+    };
+    auto emit_c = [&]() {
+        out.push_back(classify[ic++]);
+        if (ic == first[bc + 1]) last_c[bc++] = pos();
+    };
+    auto emit_p = [&]() {
+        out.push_back(pair[ip++]);
+        if (ip == first[bp + 1]) ++bp;
+    };
+    while (out.size() < total) {
+        const bool p_ready = ip < pair.size() && bp < bc;            // its CLASSIFY items are all queued
+        const bool c_ready = ic < classify.size() && bc < bm;        // its MARK items are all queued
+        if (p_ready && last_c[bp] + lag <= pos()) emit_p();
+        else if (c_ready && last_m[bc] + lag <= pos()) emit_c();
+        else if (im < mark.size() && im < ic + 2 * lag) emit_m();
+        else if (is < single.size()) out.push_back(single[is++]);
+        else if (c_ready) emit_c();
+        else if (p_ready) emit_p();
+        else emit_m();
+    }
+}
+
 }  // namespace rz
 
 struct rz_batch_plan {
@@ -408,8 +470,16 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
     if (TILE > 8192) return RZ_ERR_INVALID_ARG;  // the tile scan holds at most 8 rounds x 32 warps
     const size_t smem = size_t(TILE / 32 + 2 * TILE) * 4;
 
+    int occ = 0;
+    cudaError_t e = cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)f, cfg.block, smem);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch plan occupancy");
+    if (occ < 1) return RZ_ERR_UNSUPPORTED;
+    const int full_grid = std::max(1, std::min(cfg.ctas_per_sm, occ) * ctx->sms);
+
     std::vector<ListRec> recs(static_cast<size_t>(nlists));
     std::vector<uint2> mark, single, classify, pair;
+    std::vector<uint32_t> groups;
     uint64_t bitmap_words = 0, list_entries = 0, cnt_words = 0;
     for (int32_t l = 0; l < nlists; ++l) {
         const rz_list_desc& d = lists[l];
@@ -440,6 +510,7 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
             bitmap_words += (uint64_t(r.k) + 31) / 32;
             list_entries += uint64_t(nch) * TILE;
             cnt_words += 2ull * nch;
+            groups.push_back(r.ngroups);
             for (uint32_t g = 0; g < r.ngroups; ++g) {
                 mark.push_back(make_uint2(uint32_t(l), (K_MARK << 28) | g));
                 classify.push_back(make_uint2(uint32_t(l), (K_CLASSIFY << 28) | g));
@@ -455,11 +526,7 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
         return recs[a.x].k > recs[b.x].k;
     });
     std::vector<uint2> queue;
-    queue.reserve(mark.size() + single.size() + classify.size() + pair.size());
-    queue.insert(queue.end(), mark.begin(), mark.end());
-    queue.insert(queue.end(), single.begin(), single.end());
-    queue.insert(queue.end(), classify.begin(), classify.end());
-    queue.insert(queue.end(), pair.begin(), pair.end());
+    order_queue(mark, single, classify, pair, groups, size_t(std::max(0, cfg.wave)) * size_t(full_grid) / 2, queue);
 
     const size_t b_lists = sizeof(ListRec) * std::max<size_t>(recs.size(), 1);
     const size_t b_queue = sizeof(uint2) * std::max<size_t>(queue.size(), 1);
@@ -474,7 +541,7 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
     void* dev = nullptr;
     RZ_CUDA_TRY(ctx, cudaMalloc(&dev, total));
     uint8_t* b = static_cast<uint8_t*>(dev);
-    cudaError_t e = recs.empty() ? cudaSuccess : cudaMemcpy(b, recs.data(), sizeof(ListRec) * recs.size(),
+    e = recs.empty() ? cudaSuccess : cudaMemcpy(b, recs.data(), sizeof(ListRec) * recs.size(),
                                                             cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !queue.empty())
         e = cudaMemcpy(b + off_queue, queue.data(), sizeof(uint2) * queue.size(), cudaMemcpyHostToDevice);
@@ -483,18 +550,11 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
         cudaFree(dev);
         return cuda_fail(ctx, e, "batch plan upload");
     }
-    int occ = 0;
-    e = cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)f, cfg.block, smem);
-    if (e != cudaSuccess || occ < 1) {
-        cudaFree(dev);
-        return e != cudaSuccess ? cuda_fail(ctx, e, "batch plan occupancy") : RZ_ERR_UNSUPPORTED;
-    }
     plan->ctx = ctx;
     plan->w = w;
     plan->cfg = cfg;
     plan->smem = smem;
-    plan->grid = std::max(1, std::min<int>(std::min(cfg.ctas_per_sm, occ) * ctx->sms, int(queue.size())));
+    plan->grid = std::max(1, std::min<int>(full_grid, int(queue.size())));
     plan->nlists = uint32_t(nlists);
     plan->nitems = uint32_t(queue.size());
     plan->dev = dev;
@@ -630,7 +690,12 @@ int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStrea
     }
     if (3 * nmark + nsingle > a->max_items || bits > a->max_bits || entries > a->max_entries || cnt > a->max_cnt)
         return RZ_ERR_UNSUPPORTED;
-    size_t q_mark = 0, q_single = nmark, q_classify = nmark + nsingle, q_pair = 2 * nmark + nsingle;
+    std::vector<uint2> mark, single, classify, pair, ordered;
+    std::vector<uint32_t> groups;
+    mark.reserve(nmark);
+    classify.reserve(nmark);
+    pair.reserve(nmark);
+    single.reserve(nsingle);
     bits = entries = cnt = 0;
     for (int l = 0; l < nlists; ++l) {
         const rz_list_desc& d = lists[l];
@@ -644,7 +709,7 @@ int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStrea
         if (!(d.k == 0 || d.k == d.n)) {
             if (nch == 1) {
                 r.span = r.ngroups = 1;
-                queue[q_single++] = make_uint2(uint32_t(l), K_SINGLE << 28);
+                single.push_back(make_uint2(uint32_t(l), K_SINGLE << 28));
             } else {
                 r.span = span_for(nch, a->cfg.span);
                 r.ngroups = (nch + r.span - 1) / r.span;
@@ -654,16 +719,21 @@ int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStrea
                 bits += (uint64_t(d.k) + 31) / 32;
                 entries += size_t(nch) * TILE;
                 cnt += 2 * size_t(nch);
+                groups.push_back(r.ngroups);
                 for (uint32_t g = 0; g < r.ngroups; ++g) {
-                    queue[q_mark++] = make_uint2(uint32_t(l), (K_MARK << 28) | g);
-                    queue[q_classify++] = make_uint2(uint32_t(l), (K_CLASSIFY << 28) | g);
-                    queue[q_pair++] = make_uint2(uint32_t(l), (K_PAIR << 28) | g);
+                    mark.push_back(make_uint2(uint32_t(l), (K_MARK << 28) | g));
+                    classify.push_back(make_uint2(uint32_t(l), (K_CLASSIFY << 28) | g));
+                    pair.push_back(make_uint2(uint32_t(l), (K_PAIR << 28) | g));
                 }
             }
         }
         recs[l] = r;
     }
-    const size_t nitems = q_pair;
+    std::sort(single.begin(), single.end(), [&](const uint2& x, const uint2& y) { return recs[x.x].k > recs[y.x].k; });
+    order_queue(mark, single, classify, pair, groups, size_t(std::max(0, a->cfg.wave)) * size_t(a->grid) / 2,
+                ordered);
+    std::copy(ordered.begin(), ordered.end(), queue);
+    const size_t nitems = ordered.size();
     if (nlists > 0)
         RZ_CUDA_TRY(ctx, cudaMemcpyAsync(a->dev, a->host, sizeof(ListRec) * size_t(nlists), cudaMemcpyHostToDevice, s));
     if (nitems)
@@ -703,7 +773,7 @@ int rz_batch_plan_create(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists,
     cudaSetDevice(ctx->device);
     rz_batch_cfg c{};
     if (cfg) c = *cfg;
-    else default_batch_cfg(ctx, elem_bytes, &c);
+    else if (!predict_batch_cfg(ctx, lists, nlists, elem_bytes, &c)) default_batch_cfg(ctx, elem_bytes, &c);
     rz_batch_plan* plan = new (std::nothrow) rz_batch_plan();
     if (!plan) return RZ_ERR_NO_MEMORY;
     const int st = plan_build(ctx, lists, nlists, elem_bytes, c, plan);

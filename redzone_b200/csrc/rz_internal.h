@@ -146,6 +146,13 @@ int clamp_cfg(const rz_ctx* ctx, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
 bool predict_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, const uint32_t* d_idx,
                  cudaStream_t s, rz_launch_cfg* cfg);
 bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* cfg);
+// The batched configuration space (rz_batch_config_space): block {128,256,512} x items {2,4,8} x
+// CTAs per SM {1,2,4} x work order {phase by phase, wavefront with kDefaultWave}.
+constexpr int kDefaultWave = 6;
+constexpr int kBatchCfgSpace = 54;
+void batch_config_space(rz_batch_cfg* out);
+// The batched configuration the attached list-mix predictor picks (false without one).
+bool predict_batch_cfg(rz_ctx* ctx, const rz_list_desc* lists, int nlists, uint32_t w, rz_batch_cfg* cfg);
 void release_extras(rz_ctx* ctx);
 // The status word (offset 0) and the device length (offset 512) of the workspace block: one
 // device-to-host copy of this many bytes brings both back.

@@ -304,7 +304,8 @@ struct rz_mlp {
 namespace rz {
 
 struct Predictor {
-    rz_mlp* mlp = nullptr;
+    rz_mlp* mlp = nullptr;        // single lists: launch configuration + partition bit
+    rz_mlp* batch_mlp = nullptr;  // list mixes: batched configuration (outputs 0..kBatchCfgSpace-1)
     float* d_feat = nullptr;  // 12 floats
     float* d_out = nullptr;   // kOut floats
 };
@@ -376,6 +377,78 @@ bool predict_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, const uint32_t
     return true;
 }
 
+// ---- list mixes (the batched kernel) -----------------------------------------------------------
+// The same network, trained separately, maps 12 features of a mix of lists to logits over the
+// batched configuration space (outputs 0..kBatchCfgSpace-1; the others are trained towards zero
+// probability and ignored). Features, computed on the host from the list sizes alone, each scaled
+// to about [0, 1]:
+//   0 log2(lists)/16   1 log2(1 + total n)/36   2 log2(1 + total k)/36   3 total k / total n
+//   4 payload bytes/32   5, 6 mean and standard deviation of log2(1 + n) over the lists (/32, /8)
+//   7 mean of k/n over the lists
+//   8-10 share of the removals in lists with k <= 256, <= 1024, <= 4096 (lists that one CTA
+//        removes whole with the smaller tiles)   11 log2(1 + largest k)/24
+void batch_config_space(rz_batch_cfg* out) {
+    int q = 0;
+    for (int b : {128, 256, 512})
+        for (int i : {2, 4, 8})
+            for (int c : {1, 2, 4})
+                for (int wave : {0, kDefaultWave}) out[q++] = rz_batch_cfg{b, i, c, 0, wave};
+}
+
+void batch_features(const rz_list_desc* lists, int nlists, uint32_t w, float* f) {
+    double tn = 0, tk = 0, mlog = 0, mlog2 = 0, mf = 0, s256 = 0, s1k = 0, s4k = 0, kmax = 0;
+    int used = 0;
+    for (int l = 0; l < nlists; ++l) {
+        const double n = double(lists[l].n), k = double(lists[l].k);
+        if (n <= 0) continue;
+        ++used;
+        tn += n;
+        tk += k;
+        const double lg = std::log2(1.0 + n);
+        mlog += lg;
+        mlog2 += lg * lg;
+        mf += k / n;
+        if (k <= 256) s256 += k;
+        if (k <= 1024) s1k += k;
+        if (k <= 4096) s4k += k;
+        kmax = std::max(kmax, k);
+    }
+    const double u = std::max(used, 1);
+    mlog /= u;
+    const double var = std::max(0.0, mlog2 / u - mlog * mlog);
+    f[0] = float(std::log2(std::max(1.0, double(nlists))) / 16.0);
+    f[1] = float(std::log2(1.0 + tn) / 36.0);
+    f[2] = float(std::log2(1.0 + tk) / 36.0);
+    f[3] = float(tn > 0 ? tk / tn : 0.0);
+    f[4] = float(w) / 32.f;
+    f[5] = float(mlog / 32.0);
+    f[6] = float(std::sqrt(var) / 8.0);
+    f[7] = float(mf / u);
+    f[8] = float(tk > 0 ? s256 / tk : 0.0);
+    f[9] = float(tk > 0 ? s1k / tk : 0.0);
+    f[10] = float(tk > 0 ? s4k / tk : 0.0);
+    f[11] = float(std::log2(1.0 + kmax) / 24.0);
+}
+
+bool predict_batch_cfg(rz_ctx* ctx, const rz_list_desc* lists, int nlists, uint32_t w, rz_batch_cfg* cfg) {
+    Predictor* pr = static_cast<Predictor*>(ctx->predictor);
+    if (!pr || !pr->batch_mlp || nlists < 1) return false;
+    float feat[kIn];
+    batch_features(lists, nlists, w, feat);
+    if (cudaMemcpy(pr->d_feat, feat, sizeof(feat), cudaMemcpyHostToDevice) != cudaSuccess) return false;
+    mlp_forward_kernel<<<1, 32>>>(pr->batch_mlp->P, pr->d_feat, nullptr, nullptr, 1, nullptr, nullptr, pr->d_out,
+                                  nullptr, nullptr);
+    float o[kOut];
+    if (cudaMemcpy(o, pr->d_out, sizeof(o), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    int best = 0;
+    for (int q = 1; q < kBatchCfgSpace; ++q)
+        if (o[q] > o[best]) best = q;
+    rz_batch_cfg space[kBatchCfgSpace];
+    batch_config_space(space);
+    *cfg = space[best];
+    return true;
+}
+
 void release_predictor(rz_ctx* ctx) {
     Predictor* pr = static_cast<Predictor*>(ctx->predictor);
     if (!pr) return;
@@ -437,6 +510,7 @@ void rz_mlp_destroy(rz_mlp* m) {
     cudaSetDevice(m->ctx->device);
     Predictor* pr = static_cast<Predictor*>(m->ctx->predictor);
     if (pr && pr->mlp == m) pr->mlp = nullptr;
+    if (pr && pr->batch_mlp == m) pr->batch_mlp = nullptr;
     cudaFree(m->P);
     cudaFree(m->scratch);
     delete m;
@@ -565,10 +639,7 @@ int rz_mlp_train(rz_mlp* m, const float* h_x, const float* h_t, int64_t nsamp, i
     return st;
 }
 
-int rz_set_predictor(rz_ctx* ctx, rz_mlp* m) {
-    if (!ctx) return RZ_ERR_INVALID_ARG;
-    std::lock_guard<std::recursive_mutex> g(ctx->mu);
-    cudaSetDevice(ctx->device);
+static int ensure_predictor(rz_ctx* ctx, Predictor** out) {
     Predictor* pr = static_cast<Predictor*>(ctx->predictor);
     if (!pr) {
         pr = new (std::nothrow) Predictor();
@@ -577,14 +648,58 @@ int rz_set_predictor(rz_ctx* ctx, rz_mlp* m) {
         cudaError_t e = cudaMalloc(&p, (kIn + kOut) * sizeof(float));
         if (e != cudaSuccess) {
             delete pr;
-            return cuda_fail(ctx, e, "rz_set_predictor");
+            return cuda_fail(ctx, e, "predictor");
         }
         pr->d_feat = static_cast<float*>(p);
         pr->d_out = pr->d_feat + kIn;
         ctx->predictor = pr;
     }
+    *out = pr;
+    return RZ_OK;
+}
+
+int rz_set_predictor(rz_ctx* ctx, rz_mlp* m) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    Predictor* pr = nullptr;
+    const int st = ensure_predictor(ctx, &pr);
+    if (st != RZ_OK) return st;
     pr->mlp = m;
     return RZ_OK;
+}
+
+int rz_set_batch_predictor(rz_ctx* ctx, rz_mlp* m) {
+    if (!ctx) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    Predictor* pr = nullptr;
+    const int st = ensure_predictor(ctx, &pr);
+    if (st != RZ_OK) return st;
+    pr->batch_mlp = m;
+    return RZ_OK;
+}
+
+int rz_batch_config_space(rz_batch_cfg* out, int32_t max) {
+    rz_batch_cfg space[kBatchCfgSpace];
+    batch_config_space(space);
+    if (out)
+        for (int q = 0; q < std::min<int>(max, kBatchCfgSpace); ++q) out[q] = space[q];
+    return kBatchCfgSpace;
+}
+
+int rz_batch_features(const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes, float* h_features12) {
+    if (!h_features12 || nlists < 0 || (nlists > 0 && !lists)) return RZ_ERR_INVALID_ARG;
+    batch_features(lists, nlists, elem_bytes, h_features12);
+    return RZ_OK;
+}
+
+int rz_predict_batch_cfg(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t elem_bytes,
+                         rz_batch_cfg* cfg) {
+    if (!ctx || !cfg || nlists < 0 || (nlists > 0 && !lists)) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return predict_batch_cfg(ctx, lists, nlists, elem_bytes, cfg) ? RZ_OK : RZ_ERR_UNSUPPORTED;
 }
 
 int rz_predict_cfg(rz_ctx* ctx, const uint32_t* d_idx, int64_t n, int64_t k, uint32_t elem_bytes, rz_launch_cfg* cfg) {
