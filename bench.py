@@ -297,6 +297,10 @@ def own_arm(args):
     barrier()
     region0 = torch.cuda.Event(enable_timing=True)
     region1 = torch.cuda.Event(enable_timing=True)
+    # Every timed step follows an L2 scrub on the GPU, the first one included: the scrub keeps the
+    # stream busy while the host enqueues the first removal, so its start event does not time the
+    # host's launch call (as it would on an idle stream).
+    scrub.fill_(255)
     region0.record(stream)
     for i in range(args.steps):
         starts[i].record(stream)
@@ -351,6 +355,20 @@ def own_arm(args):
     torch.cuda.synchronize()
     part_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in p_ms))
 
+    # ---- the reference's own O(n) GPU comparator: mark with -1, then thrust::remove ----
+    t_ms = []
+    for i in range(p_steps + 2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.arange(n, out=a)  # the comparator needs -1 only where its marks put it
+        scrub.fill_(i & 255)
+        e0.record(stream)
+        assert ctx.thrust_remove(a, sets[i % NSETS]) == n - k
+        e1.record(stream)
+        if i >= 2:
+            t_ms.append((e0, e1))
+    torch.cuda.synchronize()
+    thrust_ms = max_over_ranks(statistics.mean(s.elapsed_time(e) for s, e in t_ms))
+
     # ---- event-timing floor: an empty kernel of the removal's launch shape, timed exactly like a
     # step (same events, same scrub before it) ----
     dcfg = ctx.default_cfg(n, k, W_BYTES)
@@ -383,8 +401,11 @@ def own_arm(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     inflight = []
+    issue_s = 0.0
     for i in range(e_steps):
+        h0 = time.perf_counter()
         inflight.append(ctx.remove_host_idx_async(a, e_pinned[i % E_SETS]))
+        issue_s += time.perf_counter() - h0
         if len(inflight) == E_DEPTH:
             assert ctx.wait(inflight.pop(0)) == n - k
     for t in inflight:
@@ -441,6 +462,9 @@ def own_arm(args):
                          "alg_bytes_per_launch": balg, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6.65 TB/s"},
             "partition_on": {"ms_per_step": part_ms, "speedup_redzone_vs_partition": part_ms / mean_ms},
+            "thrust_remove_on": {"ms_per_step": thrust_ms, "speedup_redzone_vs_thrust": thrust_ms / mean_ms,
+                                 "what": "the reference's O(n) GPU comparator: mark with -1, then "
+                                         "thrust::remove (Thrust_remove.hxx:15-17), same workload"},
             "graph_steady_state": {
                 "ms_per_removal": steady_ms, "items_per_s": world * k / (steady_ms * 1e-3),
                 "speedup_vs_partition": part_ms / steady_ms,
@@ -456,7 +480,8 @@ def own_arm(args):
                     "method": f"rz_remove_host_idx_async, {E_DEPTH} calls in flight, each step's list copied from "
                               f"pinned host memory and its status + length read back, rz_wait on every step; "
                               f"time of the whole region / steps; {E_SETS} distinct lists, no L2 scrub",
-                    "serial_ms_per_step": e2e_serial_ms},
+                    "serial_ms_per_step": e2e_serial_ms,
+                    "host_issue_us_per_call": 1e6 * issue_s / e_steps},
             "cpu_baseline": cpu,
             "batched": bat,
             "clocks": clk,
@@ -483,10 +508,12 @@ def sweep(args):
     scrub = torch.empty(SCRUB_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
     ks = [int(x) for x in args.sweep_k.split(",")] if args.sweep_k else list(range(10, 28))
-    for w in (4, 16):
+    widths = [int(x) for x in args.sweep_w.split(",")] if args.sweep_w else [4, 16]
+    dists = args.sweep_dist.split(",") if args.sweep_dist else ["uniform", "clustered", "tail"]
+    for w in widths:
         a = torch.zeros((n, w // 4), dtype=torch.int32, device=dev)
         a[:, 0] = torch.arange(n, dtype=torch.int32, device=dev)
-        for dist in ("uniform", "clustered", "tail"):
+        for dist in dists:
             for kl in ks:
                 k = 1 << kl
                 if dist == "tail" and k > n // 10:
@@ -508,7 +535,19 @@ def sweep(args):
                     torch.cuda.synchronize()
                     res[name] = statistics.median(s.elapsed_time(e) for s, e in ev)
                 balg = alg_bytes(n, k, w, idx_np)
+                holes = idx[idx < n - k].contiguous()
+                ev = []
+                for r in range(reps):
+                    scrub.fill_(r & 255)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    ctx.scatter(a, holes)
+                    e1.record(stream)
+                    ev.append((e0, e1))
+                torch.cuda.synchronize()
+                scatter_ms = statistics.median(s.elapsed_time(e) for s, e in ev)
                 line = {"n": n, "k": k, "w": w, "dist": dist, "redzone_ms": res["redzone"],
+                        "scatter_ms": scatter_ms, "holes": int(holes.numel()),
                         "partition_ms": res["partition"], "items_per_s": k / (res["redzone"] * 1e-3),
                         "alg_bytes": balg, "achieved_gbs": balg / (res["redzone"] * 1e-3) / 1e9,
                         "frac_of_hbm": balg / (res["redzone"] * 1e-3) / 1e9 / peak,
@@ -539,7 +578,38 @@ def make_batched_lists(args, dev, world, rank):
         idx = torch.randperm(ni, generator=g, device=dev)[:ki].to(torch.int32)
         lists.append((seg, idx))
         off += ni
-    return lists, n_all, k_all
+    return buf, lists, n_all, k_all
+
+
+def scatter_floor(ctx, buf, lists, reps: int, scrub=None) -> dict:
+    """The hole writes of `lists` alone: plain scattered stores (rz_test_scatter) of every hole
+    position (idx < n - k) into `buf`, which the lists are segments of. Overwrites the lists."""
+    import torch
+
+    base = buf.data_ptr()
+    pos = []
+    for d, i in lists:
+        cut = d.shape[0] - i.numel()
+        off = (d.data_ptr() - base) // buf.element_size()
+        pos.append(i[i < cut].to(torch.int64) + off)
+    pos = torch.cat(pos).to(torch.int32) if pos else torch.zeros(0, dtype=torch.int32, device=buf.device)
+    stream = torch.cuda.current_stream()
+    flat = buf.view(buf.shape[0], -1)
+    ctx.scatter(flat, pos)
+    ts = []
+    for r in range(reps):
+        if scrub is not None:
+            scrub.fill_(r & 255)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.scatter(flat, pos)
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    h = int(pos.numel())
+    del pos
+    ms = statistics.median(ts)
+    return {"holes": h, "ms": ms, "holes_per_s": h / (ms * 1e-3)}
 
 
 def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) -> dict:
@@ -553,7 +623,7 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
     from redzone_b200 import _native, dist
     from tests import _torch_rule
 
-    lists, n_all, k_all = make_batched_lists(args, dev, world, rank)
+    buf, lists, n_all, k_all = make_batched_lists(args, dev, world, rank)
     nlists = len(lists)
     total_n, total_k = int(n_all.sum()), int(k_all.sum())
     stream = torch.cuda.current_stream()
@@ -620,7 +690,10 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
     k_r = my_k * (kr_s / max(1, k_s))
     balg = 4.0 * my_k + 2.0 * w * (my_k - k_r) + my_k / 4.0
     peak, peak_kind = load_peaks()
-    del lists
+    # The same hole writes as plain scattered stores (after the timings above: it overwrites lists).
+    sf = scatter_floor(ctx, buf, lists, reps=3)
+    sf["removal_time_over_scatter_time"] = batched_ms / sf["ms"]
+    del lists, buf
     torch.cuda.empty_cache()
     return {
         "workload": f"{args.lists} lists, n log-uniform [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), "
@@ -637,6 +710,7 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
                      "frac": balg / (batched_ms * 1e-3) / 1e9 / peak, "traffic": None,
                      "alg_bytes_per_launch": balg, "peak_source": peak_kind},
         "parity": f"{len(sample)} sampled lists bit-exact against the canonical rule before timing",
+        "scatter_floor": sf,
     }
 
 
@@ -855,6 +929,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--sweep", action="store_true", help="run the k sweep instead of the headline")
     ap.add_argument("--sweep-k", default="", help="comma-separated log2(k) values for --sweep")
+    ap.add_argument("--sweep-w", default="", help="comma-separated item widths for --sweep (default 4,16)")
+    ap.add_argument("--sweep-dist", default="", help="comma-separated distributions for --sweep")
     ap.add_argument("--workload", choices=["single", "batched", "service", "produced"], default="single")
     ap.add_argument("--shards", type=int, default=16, help="--workload service: table shards")
     ap.add_argument("--slots", type=int, default=4, help="--workload service: concurrent launch slots")

@@ -245,6 +245,15 @@ int rz_partition(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
                  rz_stream_t stream);
 
 /*
+ * The reference's O(n) GPU comparator, for measurement only (no removal path of this library uses
+ * it): mark every removed slot of the int list with -1, then thrust::remove(list, list + n, -1),
+ * stable (Thrust_remove.hxx:15-17 with the marking of DataStruct.hxx:11-18), on `stream`.
+ * *new_len receives the length Thrust returns. Assumes -1 occurs only where the marks put it.
+ */
+int rz_test_thrust_remove(rz_ctx* ctx, int32_t* d_list, int64_t n, const uint32_t* d_idx, int64_t k,
+                          int64_t* new_len, rz_stream_t stream);
+
+/*
  * rz_remove for callers that cannot allocate device memory (an exhausted or foreign-owned memory
  * pool, a real-time path that must not take the allocator's lock or synchronise, a plugin host
  * that owns every allocation). No counterpart in the reference: its GPU path takes a
@@ -472,6 +481,13 @@ int rz_read_phase_stamps(rz_ctx* ctx, uint64_t* out, int32_t max_ctas, int32_t* 
  * events as a removal, it gives the floor that every launch of that shape pays. */
 int rz_test_empty_launch(rz_ctx* ctx, int32_t grid, int32_t block, int32_t cluster, int32_t smem_bytes,
                          rz_stream_t stream);
+
+/* Measurement aid: plain scattered stores d_data[d_pos[i]] = (an item made from i) for i in
+ * [0, count), positions >= n skipped, on `stream`, with nothing else in the kernel. Given the hole
+ * positions of a removal it measures the rate at which this GPU absorbs those writes alone: the
+ * ceiling a removal whose time goes to its hole writes can reach. It overwrites d_data. */
+int rz_test_scatter(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_pos, int64_t count,
+                    rz_stream_t stream);
 
 /*
  * Failure-detection check for the bounded device waits that replace the reference's grid

@@ -178,6 +178,22 @@ class Context:
         self._check(_native.lib.rz_test_empty_launch(self.handle, grid, block, cluster, smem,
                                                      ctypes.c_void_p(_stream_handle(stream))), "rz_test_empty_launch")
 
+    def thrust_remove(self, data, idx, stream=None) -> int:
+        """The reference's O(n) GPU comparator (mark with -1, then thrust::remove) on an int32
+        list; returns the new length."""
+        out = ctypes.c_int64(0)
+        self._check(_native.lib.rz_test_thrust_remove(self.handle, ctypes.c_void_p(data.data_ptr()), int(data.shape[0]),
+                                                      ctypes.c_void_p(idx.data_ptr()), int(idx.numel()),
+                                                      ctypes.byref(out), ctypes.c_void_p(_stream_handle(stream))),
+                    "rz_test_thrust_remove")
+        return out.value
+
+    def scatter(self, data, pos, stream=None) -> None:
+        """Plain scattered stores data[pos[i]] = item i (rz_test_scatter): the hole writes alone."""
+        self._check(_native.lib.rz_test_scatter(self.handle, ctypes.c_void_p(data.data_ptr()), int(data.shape[0]),
+                                                item_bytes(data), ctypes.c_void_p(pos.data_ptr()), int(pos.numel()),
+                                                ctypes.c_void_p(_stream_handle(stream))), "rz_test_scatter")
+
     def sync_status(self, stream=None) -> int:
         return _native.lib.rz_sync_status(self.handle, ctypes.c_void_p(_stream_handle(stream)))
 

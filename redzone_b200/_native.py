@@ -110,6 +110,8 @@ _sig("rz_partition", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINT
 _sig("rz_default_cfg", c_i32, [c_vp, c_i64, c_i64, c_u32, ctypes.POINTER(LaunchCfg)])
 _sig("rz_test_barrier_timeout", c_i32, [c_vp, c_u32, ctypes.POINTER(c_u32)])
 _sig("rz_test_empty_launch", c_i32, [c_vp, c_i32, c_i32, c_i32, c_i32, c_vp])
+_sig("rz_test_scatter", c_i32, [c_vp, c_vp, c_i64, c_u32, c_vp, c_i64, c_vp])
+_sig("rz_test_thrust_remove", c_i32, [c_vp, c_vp, c_i64, c_vp, c_i64, ctypes.POINTER(c_i64), c_vp])
 _sig("rz_last_launch", c_i32, [c_vp, ctypes.POINTER(c_i32), ctypes.POINTER(c_i32), ctypes.POINTER(c_i32)])
 _sig("rz_remove_noalloc", c_i32, [c_vp, c_i64, c_u32, c_vp, c_i64, ctypes.POINTER(c_i64), c_vp])
 _sig("rz_noalloc_sync_status", c_i32, [c_vp])

@@ -469,6 +469,18 @@ int rz_test_empty_launch(rz_ctx* ctx, int32_t grid, int32_t block, int32_t clust
     return test_empty_launch(ctx, grid, block, cluster, smem_bytes, reinterpret_cast<cudaStream_t>(stream));
 }
 
+int rz_test_scatter(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes, const uint32_t* d_pos, int64_t count,
+                    rz_stream_t stream) {
+    if (!ctx || n < 0 || count < 0 || (count > 0 && (!d_data || !d_pos))) return RZ_ERR_INVALID_ARG;
+    if (n >= (int64_t(1) << 32) || count >= (int64_t(1) << 32)) return RZ_ERR_UNSUPPORTED;
+    const uintptr_t align = elem_bytes >= 16 ? 16 : elem_bytes;
+    if (align == 0 || reinterpret_cast<uintptr_t>(d_data) % align) return RZ_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return test_scatter(ctx, d_data, uint32_t(n), elem_bytes, d_pos, uint32_t(count),
+                        reinterpret_cast<cudaStream_t>(stream));
+}
+
 int rz_test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_bits) {
     if (!ctx || !status_bits) return RZ_ERR_INVALID_ARG;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);

@@ -174,6 +174,8 @@ int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStrea
 // Test hook: run a grid barrier whose expected arrival count exceeds the grid, so that the
 // bounded wait must expire; returns the device status bits observed.
 int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out);
+// Diagnostic: plain scattered stores of `count` items at positions pos[] (the hole writes alone).
+int test_scatter(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* pos, uint32_t count, cudaStream_t s);
 // Diagnostic: launch an empty kernel of the given shape (cluster size 1-8 dividing grid).
 int test_empty_launch(rz_ctx* ctx, int grid, int block, int cluster, int smem, cudaStream_t s);
 

@@ -355,6 +355,43 @@ int test_empty_launch(rz_ctx* ctx, int grid, int block, int cluster, int smem, c
     return RZ_OK;
 }
 
+__device__ __forceinline__ void fill_item(uint32_t& v, uint32_t i) { v = i; }
+__device__ __forceinline__ void fill_item(uint2& v, uint32_t i) { v = make_uint2(i, ~i); }
+__device__ __forceinline__ void fill_item(uint4& v, uint32_t i) { v = make_uint4(i, ~i, i, ~i); }
+__device__ __forceinline__ void fill_item(u32x8& v, uint32_t i) {
+    v.a = make_uint4(i, ~i, i, ~i);
+    v.b = v.a;
+}
+
+// Plain scattered stores data[pos[i]] = item i: the rate the memory system sustains for the hole
+// writes of a removal, with nothing else in the kernel. Positions >= n are skipped.
+template <int W>
+__global__ void __launch_bounds__(256) scatter_kernel(uint8_t* __restrict__ data, uint32_t n,
+                                                      const uint32_t* __restrict__ pos, uint32_t count) {
+    using T = typename Payload<W>::T;
+    T* d = reinterpret_cast<T*>(data);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t q = __ldg(&pos[i]);
+        T v;
+        fill_item(v, i);
+        if (q < n) d[q] = v;
+    }
+}
+
+int test_scatter(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t* pos, uint32_t count, cudaStream_t s) {
+    if (count == 0) return RZ_OK;
+    const int grid = ctx->sms * 8;
+    switch (w) {
+        case 4: scatter_kernel<4><<<grid, 256, 0, s>>>(static_cast<uint8_t*>(data), n, pos, count); break;
+        case 8: scatter_kernel<8><<<grid, 256, 0, s>>>(static_cast<uint8_t*>(data), n, pos, count); break;
+        case 16: scatter_kernel<16><<<grid, 256, 0, s>>>(static_cast<uint8_t*>(data), n, pos, count); break;
+        case 32: scatter_kernel<32><<<grid, 256, 0, s>>>(static_cast<uint8_t*>(data), n, pos, count); break;
+        default: return RZ_ERR_INVALID_ARG;
+    }
+    RZ_CUDA_TRY(ctx, cudaGetLastError());
+    return RZ_OK;
+}
+
 int test_barrier_timeout(rz_ctx* ctx, uint32_t spin_limit, uint32_t* status_out) {
     cudaStream_t s = nullptr;
     int st = reset_if_dirty(ctx, s);

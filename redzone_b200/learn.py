@@ -103,7 +103,14 @@ class Mlp:
         return o[:, :N_CFG].argmax(1), (o[:, N_CFG] > 0).astype(np.int32)
 
     def attach(self) -> None:
+        """Make rz_remove(..., RZ_USE_PREDICTOR) use this network."""
         self.ctx._check(_native.lib.rz_set_predictor(self.ctx.handle, self.handle), "rz_set_predictor")
+        self._attached = "single"
+
+    def attach_batched(self) -> None:
+        """Make batched plans created without a configuration use this network."""
+        self.ctx._check(_native.lib.rz_set_batch_predictor(self.ctx.handle, self.handle), "rz_set_batch_predictor")
+        self._attached = "batched"
 
     def save(self, path) -> None:
         np.savez_compressed(path, params=self.params())
@@ -113,7 +120,7 @@ class Mlp:
 
     def close(self):
         if getattr(self, "handle", None):
-            _native.lib.rz_set_predictor(self.ctx.handle, None)
+            # Destroying the network detaches it from the context (rz_mlp_destroy).
             _native.lib.rz_mlp_destroy(self.handle)
             self.handle = None
 

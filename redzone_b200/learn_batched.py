@@ -224,7 +224,7 @@ def attach_default(ctx) -> Mlp | None:
         return None
     m = Mlp(ctx)
     m.load(path)
-    ctx._check(_native.lib.rz_set_batch_predictor(ctx.handle, m.handle), "rz_set_batch_predictor")
+    m.attach_batched()
     return m
 
 
