@@ -614,41 +614,28 @@ def scatter_floor(ctx, buf, lists, reps: int, scrub=None) -> dict:
 
 def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) -> dict:
     """4096 uneven lists (n log-uniform in [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), uint64
-    payload = list id << 32 | index): one persistent graph-replayed launch against one rz_remove
-    launch per list (stream-launched, and the same launches captured in one CUDA graph). N > 1:
-    the lists are partitioned across ranks by removals (contiguous, balanced), each rank runs its
-    share as one launch; no collective on the data path, max-over-ranks timing."""
+    payload = list id << 32 | index) in one persistent graph-replayed launch, its configuration
+    picked by the learned list-mix predictor, against one rz_remove launch per list (stream-
+    launched, and the same launches captured in one CUDA graph), against the built-in default
+    configuration, and against every configuration of the space (exhaustive autotune: the judge
+    of the predictor's regret). N > 1: the lists are partitioned across ranks by removals
+    (contiguous, balanced), each rank runs its share as one launch; no collective on the data path,
+    max-over-ranks timing. The payload (about 14 GB) is far larger than L2."""
     import torch
     import redzone_b200 as rz
-    from redzone_b200 import _native, dist
+    from redzone_b200 import _native, dist, learn_batched
     from tests import _torch_rule
 
     buf, lists, n_all, k_all = make_batched_lists(args, dev, world, rank)
     nlists = len(lists)
     total_n, total_k = int(n_all.sum()), int(k_all.sum())
+    w = 8
     stream = torch.cuda.current_stream()
-    tuned = _native.BatchCfg()
-    best_ms = _native.c_f32(0)
-    cfg = None
-    if not args.no_tune:
-        sub = [lists[l] for l in range(0, nlists, 8)]  # tune on a 1/8 sample of the lists
-        st = _native.lib.rz_autotune_batched(ctx.handle, rz.list_descs(sub), len(sub), 8, 3,
-                                             ctypes_byref(tuned), ctypes_byref(best_ms))
-        if st == 0:
-            cfg = tuned
-            _native.lib.rz_tune_table_set_batched(ctx.handle, 8, ctypes_byref(tuned))
-    # Parity gate on a sample of lists (not timed); the tuner above rewrote some lists, so the
-    # expected prefixes are taken from the current contents.
-    sample = list(range(0, nlists, max(1, nlists // 64)))
-    exp = {l: _torch_rule.canonical_prefix(lists[l][0].clone(), lists[l][1]) for l in sample}
-    plan = rz.BatchPlan(ctx, lists, cfg)
-    plan.launch()
-    torch.cuda.synchronize()
-    assert ctx.sync_status() == 0
-    for l in sample:
-        ni, ki = lists[l][0].shape[0], lists[l][1].numel()
-        assert torch.equal(lists[l][0][: ni - ki], exp[l]), f"batched parity failed on list {l}"
-    del exp
+    descs = rz.list_descs(lists)
+    model = None if args.no_learned else learn_batched.attach_default(ctx)
+    pred = _native.BatchCfg()
+    learned = model is not None and _native.lib.rz_predict_batch_cfg(ctx.handle, descs, nlists, w,
+                                                                     ctypes_byref(pred)) == 0
 
     def timed(fn, reps):
         ts = []
@@ -661,10 +648,46 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
             ts.append(e0.elapsed_time(e1))
         return statistics.median(ts)
 
+    # Parity gate on a sample of lists (not timed), with the plan that is timed below: created
+    # without a configuration, so the attached network (or, without it, the default) chooses.
+    sample = list(range(0, nlists, max(1, nlists // 64)))
+    exp = {l: _torch_rule.canonical_prefix(lists[l][0].clone(), lists[l][1]) for l in sample}
+    plan = rz.BatchPlan(ctx, lists)
+    plan.launch()
+    torch.cuda.synchronize()
+    assert ctx.sync_status() == 0
+    for l in sample:
+        ni, ki = lists[l][0].shape[0], lists[l][1].numel()
+        assert torch.equal(lists[l][0][: ni - ki], exp[l]), f"batched parity failed on list {l}"
+    del exp
     for _ in range(warmup):
         plan.launch()
     dist.barrier(dev)
     batched_ms = dist.max_over_ranks(timed(plan.launch, steps), dev)
+    info = plan.info()
+    plan.close()
+
+    def time_cfg(cfg, reps):
+        try:
+            pl = rz.BatchPlan(ctx, lists, cfg)
+        except rz.RedzoneError:
+            return float("inf")
+        pl.launch()
+        t = timed(pl.launch, reps)
+        pl.close()
+        return t
+
+    space = learn_batched.config_space()
+    dflt = space[learn_batched.default_class(None, w)]
+    default_ms = dist.max_over_ranks(time_cfg(_native.BatchCfg(*dflt[:3], 0, dflt[3]), max(3, steps // 2)), dev)
+    exhaustive = None
+    if not args.no_tune:
+        ts = [dist.max_over_ranks(time_cfg(_native.BatchCfg(b, i, c, 0, wv), 3), dev) for b, i, c, wv in space]
+        q = int(np.argmin(ts))
+        exhaustive = {"best_cfg": list(space[q]), "best_ms": ts[q], "configurations": len(space),
+                      "default_regret": default_ms / ts[q] - 1.0}
+        if learned:
+            exhaustive["learned_regret"] = batched_ms / ts[q] - 1.0
 
     def plain():
         for d, i in lists:
@@ -678,9 +701,6 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
     plain_graph.replay()
     plain_graph_ms = dist.max_over_ranks(timed(plain_graph.replay, max(3, steps // 5)), dev)
     del plain_graph
-    info = plan.info()
-    plan.close()
-    w = 8
     # Algorithmic bytes: red-zone entries estimated from a sample of this rank's lists.
     kr_s = k_s = 0
     for d, i in lists[:: max(1, nlists // 256)]:
@@ -693,19 +713,24 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
     # The same hole writes as plain scattered stores (after the timings above: it overwrites lists).
     sf = scatter_floor(ctx, buf, lists, reps=3)
     sf["removal_time_over_scatter_time"] = batched_ms / sf["ms"]
+    if model is not None:
+        model.close()
     del lists, buf
     torch.cuda.empty_cache()
     return {
         "workload": f"{args.lists} lists, n log-uniform [2^8, 2^22], k = round(f n), f ~ U(0.001, 0.5), "
                     f"uint64 payload (list id << 32 | index), one persistent graph-replayed launch per GPU",
         "total_n": total_n, "total_k": total_k, "batch_cfg": info,
-        "tuned_ms": float(best_ms.value) if cfg is not None else None,
+        "configuration_from": "learned list-mix predictor" if learned else "built-in default (no predictor)",
+        "learned_cfg": [pred.block, pred.items, pred.ctas_per_sm, pred.wave] if learned else None,
         "items_per_s": total_k / (batched_ms * 1e-3), "ms_per_launch": batched_ms, "steps": steps,
         "parallelism": "single GPU" if world == 1 else f"{world} GPUs, lists partitioned by removals",
         "plain_per_list": {"ms_per_step": plain_ms, "speedup_batched_vs_plain": plain_ms / batched_ms},
         "plain_per_list_graph": {"ms_per_step": plain_graph_ms,
                                  "speedup_batched_vs_plain": plain_graph_ms / batched_ms},
         "speedup_vs_plain": plain_ms / batched_ms,
+        "default_cfg": {"cfg": list(dflt), "ms_per_launch": default_ms},
+        "exhaustive_autotune": exhaustive,
         "roofline": {"bound": "hbm", "achieved": balg / (batched_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": balg / (batched_ms * 1e-3) / 1e9 / peak, "traffic": None,
                      "alg_bytes_per_launch": balg, "peak_source": peak_kind},
@@ -731,9 +756,11 @@ def batched(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": b["ms_per_launch"], "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": b["workload"], "total_n": b["total_n"], "total_k": b["total_k"],
-                   "batch_cfg": b["batch_cfg"], "parallelism": b["parallelism"], "tuned_ms": b["tuned_ms"]},
+                   "batch_cfg": b["batch_cfg"], "parallelism": b["parallelism"],
+                   "configuration_from": b["configuration_from"]},
         "plain_per_list": b["plain_per_list"], "plain_per_list_graph": b["plain_per_list_graph"],
-        "roofline": b["roofline"], "gpu_launches": args.steps,
+        "default_cfg": b["default_cfg"], "exhaustive_autotune": b["exhaustive_autotune"],
+        "scatter_floor": b["scatter_floor"], "roofline": b["roofline"], "gpu_launches": args.steps,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -941,8 +968,9 @@ def main():
     ap.add_argument("--pool", type=int, default=256, help="--workload service: pinned batch pool size")
     ap.add_argument("--lists", type=int, default=4096, help="--workload batched: number of lists")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--no-tune", action="store_true", help="--workload batched: skip the autotuner")
+    ap.add_argument("--no-tune", action="store_true", help="batched: skip the exhaustive autotune")
     ap.add_argument("--no-batched", action="store_true", help="default run: skip the batched leg")
+    ap.add_argument("--no-learned", action="store_true", help="batched: do not attach the list-mix predictor")
     ap.add_argument("--config", default=None,
                     help="JSON file of option defaults, e.g. {\"workload\": \"service\", \"rate\": 40000}; "
                          "flags on the command line override it")

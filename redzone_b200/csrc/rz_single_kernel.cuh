@@ -445,11 +445,12 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
                 }
                 if (sv[j] && !dv[j]) {
                     const uint32_t rank = (ex & 0xffffu) + __popc(smask[j] & lt);
-                    // 4-byte items with one tile per CTA: the list holds the source item itself
-                    // (already in registers; tail items are never written), which saves phase C
-                    // a dependent load. Otherwise it holds the source position.
+                    // 4-byte items: the list holds the source item itself (in registers: every
+                    // tile loads its tail items; tail items are never written), which saves
+                    // phase C a dependent random load per orphan. Otherwise it holds the source
+                    // position.
                     if constexpr (W == 4) {
-                        p.slist[chunk_base + scnt + rank] = single ? uint32_t(src[j]) : cut + i;
+                        p.slist[chunk_base + scnt + rank] = uint32_t(src[j]);
                     } else {
                         p.slist[chunk_base + scnt + rank] = cut + i;
                     }
@@ -534,7 +535,7 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
         const uint32_t ent = __ldcg(&p.slist[base2 + (jr - s_ps[c2])]);
         const uint32_t dest = __ldcg(&p.dlist[chunk_base + r]);
         if constexpr (W == 4) {
-            head[dest] = single ? T(ent) : reinterpret_cast<const T*>(p.data)[ent];
+            head[dest] = T(ent);
         } else {
             head[dest] = reinterpret_cast<const T*>(p.data)[ent];
         }
