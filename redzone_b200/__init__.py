@@ -44,6 +44,11 @@ def item_bytes(t) -> int:
 def _stream_handle(stream) -> int | None:
     import torch
     if stream is None:
+        # torch's current stream of the current device, as a raw handle (cheaper than building a
+        # torch.cuda.Stream object on every call)
+        raw = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+        if raw is not None:
+            return raw(torch.cuda.current_device())
         stream = torch.cuda.current_stream()
     return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
 
@@ -155,15 +160,14 @@ class Context:
     def remove_host_idx_async(self, data, h_idx, flags: int = 0, stream=None) -> int:
         """Pipelined host-index removal (rz_remove_host_idx_async): returns a ticket at once;
         collect the result with ``wait(ticket)``. ``h_idx`` must stay unchanged until then."""
-        n = int(data.shape[0])
+        n = data.shape[0]
         if hasattr(h_idx, "data_ptr"):
-            ptr, k = h_idx.data_ptr(), int(h_idx.numel())
+            ptr, k = h_idx.data_ptr(), h_idx.numel()
         else:
-            ptr, k = h_idx.ctypes.data, int(h_idx.size)
+            ptr, k = h_idx.ctypes.data, h_idx.size
         t = ctypes.c_uint64(0)
-        st = _native.lib.rz_remove_host_idx_async(self.handle, ctypes.c_void_p(data.data_ptr()), n, item_bytes(data),
-                                                  ctypes.c_void_p(ptr), k, flags,
-                                                  ctypes.c_void_p(_stream_handle(stream)), ctypes.byref(t))
+        st = _native.lib.rz_remove_host_idx_async(self.handle, data.data_ptr(), n, item_bytes(data), ptr, k, flags,
+                                                  _stream_handle(stream), ctypes.byref(t))
         self._check(st, "rz_remove_host_idx_async")
         return t.value
 

@@ -480,6 +480,7 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
     std::vector<ListRec> recs(static_cast<size_t>(nlists));
     std::vector<uint2> mark, single, classify, pair;
     std::vector<uint32_t> groups;
+    plan->total_k = 0;
     uint64_t bitmap_words = 0, list_entries = 0, cnt_words = 0;
     for (int32_t l = 0; l < nlists; ++l) {
         const rz_list_desc& d = lists[l];
@@ -585,6 +586,21 @@ static int plan_enqueue(rz_batch_plan* plan, cudaStream_t s) {
 }
 
 bool default_batch_cfg(const rz_ctx* ctx, uint32_t w, rz_batch_cfg* cfg);  // rz_autotune.cpp
+
+// The default (or tuned) configuration, with items and then block raised until every list fits
+// in kMaxTilesPerList tiles (a plan created without a configuration must not fail on long lists).
+static void default_fitting(const rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t w,
+                            rz_batch_cfg* cfg) {
+    default_batch_cfg(ctx, w, cfg);
+    int64_t kmax = 0;
+    for (int32_t l = 0; l < nlists; ++l)
+        if (lists[l].k < lists[l].n) kmax = std::max<int64_t>(kmax, lists[l].k);
+    while (int64_t(cfg->block) * cfg->items * kMaxTilesPerList < kmax) {
+        if (cfg->items < 8) cfg->items *= 2;
+        else if (cfg->block < 512) cfg->block *= 2;
+        else break;
+    }
+}
 
 // ------------------------------------------------------------------------------------------------
 // Arenas: batched launches without per-launch allocation (used by the streaming service). An
@@ -772,11 +788,19 @@ int rz_batch_plan_create(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists,
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
     rz_batch_cfg c{};
+    bool predicted = false;
     if (cfg) c = *cfg;
-    else if (!predict_batch_cfg(ctx, lists, nlists, elem_bytes, &c)) default_batch_cfg(ctx, elem_bytes, &c);
+    else if (!(predicted = predict_batch_cfg(ctx, lists, nlists, elem_bytes, &c)))
+        default_fitting(ctx, lists, nlists, elem_bytes, &c);
     rz_batch_plan* plan = new (std::nothrow) rz_batch_plan();
     if (!plan) return RZ_ERR_NO_MEMORY;
-    const int st = plan_build(ctx, lists, nlists, elem_bytes, c, plan);
+    int st = plan_build(ctx, lists, nlists, elem_bytes, c, plan);
+    if (st == RZ_ERR_UNSUPPORTED && predicted) {
+        // The network's choice cannot plan these lists (a tile too small for the longest one):
+        // fall back to the default with a tile that fits.
+        default_fitting(ctx, lists, nlists, elem_bytes, &c);
+        st = plan_build(ctx, lists, nlists, elem_bytes, c, plan);
+    }
     if (st != RZ_OK) {
         delete plan;
         return st;

@@ -43,3 +43,22 @@ def test_soft_targets_ignore_infeasible_configurations():
     assert t.shape == (1, 64)
     assert abs(t[0].sum() - 1) < 1e-5 and t[0, 2] == 0 and t[0, 54:].sum() == 0
     assert t[0, 0] > t[0, 1] > t[0, 3]
+
+
+def test_shipped_batch_predictor_beats_the_method_without_it():
+    """Held-out list mixes, every configuration timed on a B200 (median of 5 launches): the
+    network's choice (CPU oracle forward of the shipped weights) is within 5 % of the exhaustive
+    best on average, better than the default configuration (the method without the network) and
+    than the best single fixed configuration, and never a configuration that cannot run the mix."""
+    from pathlib import Path
+    from oracle import mlp_ref
+    root = Path(__file__).resolve().parent.parent
+    p = np.load(root / "redzone_b200" / "data" / "batch_predictor.npz")["params"].astype(np.float64)
+    h = np.load(root / "tests" / "golden" / "batch_predictor_heldout.npz")
+    assert [tuple(x) for x in h["space"]] == learn_batched.config_space()
+    _, _, out = mlp_ref.forward(p, h["X"].astype(np.float64))
+    pred = out[:, : learn_batched.n_cfg()].argmax(1)
+    rep = learn_batched.evaluate(pred, h["T"], h["default_cls"])
+    assert rep["infeasible_predictions"] == 0 and rep["default_infeasible"] == 0
+    assert rep["regret_mean"] <= 0.05, rep
+    assert rep["regret_mean"] < rep["default_regret_mean"] and rep["regret_mean"] < rep["best_fixed_regret_mean"]

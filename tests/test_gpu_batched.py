@@ -57,13 +57,15 @@ def test_batched_matches_per_list_oracle(ctx, words):
         assert np.array_equal(got[: n - k], exp[: n - k]), (words, l, n, k)
 
 
-@pytest.mark.parametrize("block,items,cps", [(128, 2, 1), (256, 8, 4), (512, 4, 2), (256, 1, 8)])
-def test_batched_configs_and_graph_replay(ctx, block, items, cps):
-    """Every tile/grid choice gives the same bits, and a second graph replay (on the compacted
-    arrays) equals applying the rule twice."""
+@pytest.mark.parametrize("block,items,cps,wave", [(128, 2, 1, 0), (256, 8, 4, 0), (512, 4, 2, 0), (256, 1, 8, 0),
+                                                  (128, 2, 1, 1), (256, 8, 4, 6), (512, 4, 2, 2), (256, 2, 4, 6)])
+def test_batched_configs_and_graph_replay(ctx, block, items, cps, wave):
+    """Every tile/grid choice and both work orders (phase by phase, wavefront with several lags)
+    give the same bits, and a second graph replay (on the compacted arrays) equals applying the
+    rule twice."""
     hosts, idxs = make_lists(3, 120, 3, 16, 2, f_hi=0.3)
     dl = to_dev(hosts, idxs)
-    plan = rz.BatchPlan(ctx, dl, _native.BatchCfg(block, items, cps, 0))
+    plan = rz.BatchPlan(ctx, dl, _native.BatchCfg(block, items, cps, 0, wave))
     plan.launch()
     torch.cuda.synchronize()
     assert ctx.sync_status() == 0
