@@ -61,7 +61,7 @@ int ensure_lists(rz_ctx* ctx, size_t k) {
     st = grow(ctx, ctx->ws.slist, cap2, k + 1, false);
     if (st != RZ_OK) return st;
     ctx->ws.list_cap = std::min(cap, cap2);
-    if (k <= kFastMaxK) return grow(ctx, ctx->ws.redlist, ctx->ws.red_cap, k + 1, false);
+    if (k <= kRedlistMaxK) return grow(ctx, ctx->ws.redlist, ctx->ws.red_cap, k + 1, false);
     return RZ_OK;
 }
 

@@ -19,6 +19,10 @@ constexpr uint32_t kSpinLimit = 1u << 22;  // polls of a bounded device wait (~0
 // entries with its arrival, and when the whole grid has at most kFastMaxRed of them each CTA
 // derives the orphan pairing from that list in shared memory (no orphan-count exchange).
 constexpr uint32_t kFastMaxK = 1u << 17;   // k bound: two k-bit maps live in shared memory
+// The grid kernel's red-list schedule goes further: its two k-bit maps take 128 KB at 2^19 (one
+// CTA per SM). Above kFastMaxK it is chosen only when uniform removals would leave at most
+// kFastMaxRed red entries (k^2 / n), since a grid with more falls back to the bitmap phases.
+constexpr uint32_t kRedlistMaxK = 1u << 19;
 constexpr uint32_t kFastMaxRed = 1024;     // red entries of the whole grid
 
 // Library scratch owned by one context. Every buffer is zero where the kernels require it on

@@ -18,7 +18,7 @@
 //     epoch-tagged words; only CTAs that own destination orphans wait for the others, prefix the
 //     counts and binary-search the owner of each source rank (instead of the reference's
 //     LoadBalance linear search, :477-524).
-//   * Red-list schedule (one tile per CTA, k <= kFastMaxK): in phase A each CTA also writes its
+//   * Red-list schedule (one tile per CTA, k <= kRedlistMaxK): in phase A each CTA also writes its
 //     red entries {i, idx[i] - cut} in i order to its region of a list and arrives with a 64-bit
 //     word tag << 32 | count. If the grid holds at most kFastMaxRed red entries, every CTA reads
 //     them all into shared memory: V (tail positions whose item is removed) and P (positions whose
@@ -134,7 +134,7 @@ static int allow_redlist_smem(rz_ctx* ctx, int w, int items) {
     std::atomic<uint64_t>& d = done[wi(w)][ii(items)];
     if (d.load() & bit) return RZ_OK;
     RZ_CUDA_TRY(ctx, cudaFuncSetAttribute((const void*)single_fn(w, items), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int(redlist_smem_bytes(kFastMaxK))));
+                                          int(redlist_smem_bytes(kRedlistMaxK))));
     d.fetch_or(bit);
     return RZ_OK;
 }
@@ -265,7 +265,9 @@ int launch_redzone(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     bool fast = false;
     size_t dsmem = 0;
     long grid = 1;
-    if (sched != RZ_SCHED_BLOCK && k <= kFastMaxK && ctx->ws.redlist && ntiles > 1) {
+    const bool few_red = k <= kFastMaxK || double(k) * double(k) <= double(kFastMaxRed) * double(n);
+    if (sched != RZ_SCHED_BLOCK && k <= kRedlistMaxK && few_red && ctx->ws.redlist && ctx->ws.red_cap > k &&
+        ntiles > 1) {
         st = allow_redlist_smem(ctx, int(w), cfg.items);
         if (st != RZ_OK) return st;
         const size_t need = redlist_smem_bytes(k);

@@ -23,7 +23,7 @@ struct SingleParams {
     unsigned long long* stamps;  // nullable: 8 globaltimer stamps per CTA
     uint32_t spin_limit;
     uint32_t validate;
-    // Red-list schedule (nullable; set only with one tile per CTA, k <= kFastMaxK and the dynamic
+    // Red-list schedule (nullable; set only with one tile per CTA, k <= kRedlistMaxK and the dynamic
     // shared memory it needs): red entries per CTA region and tagged per-CTA entry counts.
     uint2* redlist;
     unsigned long long* arrive64;

@@ -499,3 +499,28 @@ def test_full_size_n_2_28(ctx, k_log2, dist):
     assert all(props.values()), props
     del a, exp
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("log2n,log2k,words,dist", [(26, 18, 1, "uniform"), (28, 19, 1, "uniform"),
+                                                    (26, 18, 4, "uniform"), (24, 19, 1, "uniform"),
+                                                    (26, 18, 1, "tail")])
+def test_redlist_schedule_beyond_2e17(ctx, log2n, log2k, words, dist):
+    """The grid kernel's red-list schedule for 2^17 < k <= 2^19 (k-bit maps of up to 128 KB in
+    shared memory; chosen when k^2/n <= 1024), and the cases that fall back to the bitmap phases
+    (more red entries: n = 2^24 with k = 2^19, tail-heavy removals) -- bit-exact against the
+    vectorised rule, with every launch configuration of the grid schedule at this size."""
+    n, k = 1 << log2n, 1 << log2k
+    a0 = torch.zeros((n, words), dtype=torch.int32, device=DEV)
+    a0[:, 0] = torch.arange(n, dtype=torch.int32, device=DEV)
+    idx = workloads.make_torch(dist, n, k, seed=log2n * 100 + log2k).contiguous()
+    exp = _torch_rule.canonical_prefix(a0, idx)
+    for cfg in [None, rz.LaunchCfg(896, 4, 2, 0, 0), rz.LaunchCfg(1024, 4, 1, 0, 0), rz.LaunchCfg(512, 8, 2, 0, 0)]:
+        a = a0.clone()
+        if cfg is None:
+            ctx.remove(a, idx, flags=rz.RZ_SYNC)
+        else:
+            ctx.remove_cfg(a, idx, cfg, flags=rz.RZ_SYNC)
+        assert torch.equal(a[: n - k], exp), (log2n, log2k, words, dist, cfg)
+        del a
+    del a0, exp
+    torch.cuda.empty_cache()
