@@ -29,7 +29,7 @@
 namespace rz {
 
 enum : uint32_t { K_MARK = 0, K_SINGLE = 1, K_CLASSIFY = 2, K_PAIR = 3 };
-constexpr uint32_t kMaxTilesPerList = 1024;
+constexpr uint32_t kMaxTilesPerList = kBatchMaxTilesPerList;
 constexpr uint32_t kNoItem = 0xffffffffu;
 
 struct ListRec {            // one per list, device-resident

@@ -153,6 +153,7 @@ bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* c
 // The batched configuration space (rz_batch_config_space): block {128,256,512} x items {2,4,8} x
 // CTAs per SM {1,2,4} x work order {phase by phase, wavefront with kDefaultWave}.
 constexpr int kDefaultWave = 6;
+constexpr uint32_t kBatchMaxTilesPerList = 1024;  // tiles one list of the batched kernel may span
 constexpr int kBatchCfgSpace = 54;
 void batch_config_space(rz_batch_cfg* out);
 // The batched configuration the attached list-mix predictor picks (false without one).

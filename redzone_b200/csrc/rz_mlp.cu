@@ -440,11 +440,19 @@ bool predict_batch_cfg(rz_ctx* ctx, const rz_list_desc* lists, int nlists, uint3
                                   nullptr, nullptr);
     float o[kOut];
     if (cudaMemcpy(o, pr->d_out, sizeof(o), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
-    int best = 0;
-    for (int q = 1; q < kBatchCfgSpace; ++q)
-        if (o[q] > o[best]) best = q;
+    // Only configurations whose tile lets the longest list fit in the batched kernel's tile limit
+    // are candidates (the others cannot plan this mix).
+    int64_t kmax = 0;
+    for (int l = 0; l < nlists; ++l)
+        if (lists[l].k < lists[l].n) kmax = std::max<int64_t>(kmax, lists[l].k);
     rz_batch_cfg space[kBatchCfgSpace];
     batch_config_space(space);
+    int best = -1;
+    for (int q = 0; q < kBatchCfgSpace; ++q) {
+        if (int64_t(space[q].block) * space[q].items * kBatchMaxTilesPerList < kmax) continue;
+        if (best < 0 || o[q] > o[best]) best = q;
+    }
+    if (best < 0) return false;
     *cfg = space[best];
     return true;
 }

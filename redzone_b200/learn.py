@@ -156,10 +156,18 @@ def soft_targets(times: np.ndarray, tau: float = 0.03) -> np.ndarray:
     return np.concatenate([p, bit[:, None]], axis=1).astype(np.float32)
 
 
-def draw_instance(rng: np.random.Generator) -> tuple[int, int, int, str]:
+def draw_instance(rng: np.random.Generator, klog: tuple[float, float] | None = None) -> tuple[int, int, int, str]:
     """(n, k, w, distribution): mixes of the n = 2^20 (k = 2^14) and n = 2^28 (k sweep, int32 and
     16-byte items) configurations, with intermediate list sizes for coverage. k reaches 2^24, where
-    the O(n) partition overtakes the O(k) removal at n = 2^28."""
+    the O(n) partition overtakes the O(k) removal at n = 2^28. With `klog` = (lo, hi), only
+    instances with log2 k in [lo, hi) are kept (the same distribution, restricted)."""
+    while True:
+        n, k, w, dist = _draw_instance(rng)
+        if klog is None or klog[0] <= math.log2(max(k, 1)) < klog[1]:
+            return n, k, w, dist
+
+
+def _draw_instance(rng: np.random.Generator) -> tuple[int, int, int, str]:
     if rng.random() < 0.15:
         n, k = 1 << 20, 1 << 14
     else:
@@ -175,7 +183,8 @@ def draw_instance(rng: np.random.Generator) -> tuple[int, int, int, str]:
     return n, min(k, n // 2), w, dist
 
 
-def collect(ctx, count: int, seed: int, reps: int = 1, log_every: int = 500):
+def collect(ctx, count: int, seed: int, reps: int = 1, log_every: int = 500,
+            klog: tuple[float, float] | None = None):
     """Features and 64 timings for `count` seeded instances (timing rewrites a scratch array)."""
     import torch
     from . import workloads
@@ -191,7 +200,7 @@ def collect(ctx, count: int, seed: int, reps: int = 1, log_every: int = 500):
     space = {c: q for q, c in enumerate(config_space())}
     t0 = time.time()
     for q in range(count):
-        n, k, w, dist = draw_instance(rng)
+        n, k, w, dist = draw_instance(rng, klog)
         idx = workloads.make_torch(dist, n, k, seed=int(rng.integers(0, 1 << 62))).contiguous()
         data = buf[: n * (w // 4)].view(n, w // 4)
         f = np.zeros(N_IN, np.float32)
@@ -258,6 +267,8 @@ def main(argv=None):
     c.add_argument("--seed", type=int, default=0)
     c.add_argument("--out", required=True)
     c.add_argument("--reps", type=int, default=1, help="timed runs per configuration (median)")
+    c.add_argument("--klog", type=float, nargs=2, default=None,
+                   help="keep only instances with log2 k in [lo, hi) (re-timing a range after a kernel change)")
     t = sub.add_parser("train")
     t.add_argument("--data", nargs="+", required=True)
     t.add_argument("--heldout", nargs="+", required=True)
@@ -274,7 +285,7 @@ def main(argv=None):
 
     ctx = rz.Context(0)
     if args.cmd == "collect":
-        X, T, meta = collect(ctx, args.count, args.seed, reps=args.reps)
+        X, T, meta = collect(ctx, args.count, args.seed, reps=args.reps, klog=args.klog)
         np.savez_compressed(args.out, X=X, T=T, meta=meta, seed=args.seed, reps=args.reps)
         print(json.dumps({"collected": int(X.shape[0]), "reps": args.reps, "out": args.out}))
         return

@@ -211,9 +211,24 @@ def soft_targets(times: np.ndarray, tau: float = 0.03) -> np.ndarray:
     return out
 
 
+def feasible_mask(X: np.ndarray) -> np.ndarray:
+    """(mixes, configurations): the configurations whose tile lets the longest list of the mix
+    (from its feature 11) fit in the batched kernel's tile limit -- the library's prediction only
+    considers those."""
+    space = np.array(config_space())
+    tile_cap = space[:, 0].astype(np.int64) * space[:, 1] * MAX_TILES_PER_LIST
+    kmax = np.array([kmax_of(x) for x in X], np.int64)
+    return tile_cap[None, :] >= kmax[:, None]
+
+
+def choose(logits: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """The library's choice from network outputs: the best feasible configuration."""
+    o = np.where(feasible_mask(X), logits[:, : n_cfg()], -np.inf)
+    return o.argmax(1)
+
+
 def predict(m: Mlp, X: np.ndarray) -> np.ndarray:
-    o = m.forward(X)
-    return o[:, : n_cfg()].argmax(1)
+    return choose(m.forward(X), X)
 
 
 def evaluate(pred: np.ndarray, T: np.ndarray, default_cls: np.ndarray) -> dict:
