@@ -271,6 +271,9 @@ def main(argv=None):
                    help="keep only instances with log2 k in [lo, hi) (re-timing a range after a kernel change)")
     t = sub.add_parser("train")
     t.add_argument("--data", nargs="+", required=True)
+    t.add_argument("--stale", nargs="*", default=[],
+                   help="data files timed before a kernel change; their rows with log2 k in --stale-klog are dropped")
+    t.add_argument("--stale-klog", type=float, nargs=2, default=None)
     t.add_argument("--heldout", nargs="+", required=True)
     t.add_argument("--epochs", type=int, default=60)
     t.add_argument("--tau", type=float, default=0.05, help="soft-target temperature (relative time)")
@@ -280,18 +283,41 @@ def main(argv=None):
     t.add_argument("--fixture", default=None,
                    help="also write the first --fixture-count held-out rows (features, timings, default class)")
     t.add_argument("--fixture-count", type=int, default=1000)
+    e = sub.add_parser("evaluate", help="regret of saved weights on held-out data")
+    e.add_argument("--weights", required=True)
+    e.add_argument("--heldout", nargs="+", required=True)
     args = ap.parse_args(argv)
     import redzone_b200 as rz
 
     ctx = rz.Context(0)
+    if args.cmd == "evaluate":
+        hold = [np.load(p) for p in args.heldout]
+        Xh = np.concatenate([p["X"] for p in hold])
+        Th = np.concatenate([p["T"] for p in hold])
+        Mh = np.concatenate([p["meta"] for p in hold])
+        m = Mlp(ctx)
+        m.load(args.weights)
+        cls, bit = m.predict(Xh)
+        dcls = np.array([default_class(ctx, *row[:3]) for row in Mh])
+        rep = evaluate(cls, bit, Th, dcls)
+        rep.update({"weights": args.weights, "heldout_seeds": [int(p["seed"]) for p in hold]})
+        print(json.dumps(rep))
+        return
     if args.cmd == "collect":
         X, T, meta = collect(ctx, args.count, args.seed, reps=args.reps, klog=args.klog)
         np.savez_compressed(args.out, X=X, T=T, meta=meta, seed=args.seed, reps=args.reps)
         print(json.dumps({"collected": int(X.shape[0]), "reps": args.reps, "out": args.out}))
         return
     parts = [np.load(p) for p in args.data]
-    X = np.concatenate([p["X"] for p in parts])
-    T = np.concatenate([p["T"] for p in parts])
+    keep = []
+    for path, p in zip(args.data, parts):
+        rows = np.ones(p["X"].shape[0], bool)
+        if path in args.stale and args.stale_klog:
+            lk = np.log2(np.maximum(p["meta"][:, 1], 1))
+            rows = ~((lk >= args.stale_klog[0]) & (lk < args.stale_klog[1]))
+        keep.append(rows)
+    X = np.concatenate([p["X"][r] for p, r in zip(parts, keep)])
+    T = np.concatenate([p["T"][r] for p, r in zip(parts, keep)])
     hold = [np.load(p) for p in args.heldout]
     Xh = np.concatenate([p["X"] for p in hold])
     Th = np.concatenate([p["T"] for p in hold])
@@ -304,6 +330,7 @@ def main(argv=None):
     dcls = np.array([default_class(ctx, *row[:3]) for row in Mh])
     rep = evaluate(cls, bit, Th, dcls)
     rep.update({"train_instances": int(X.shape[0]), "heldout_instances": int(Xh.shape[0]), "final_loss": loss,
+                "dropped_stale_instances": int(sum((~r).sum() for r in keep)),
                 "train_seconds": train_s, "epochs": args.epochs, "tau": args.tau, "lr": args.lr,
                 "train_seeds": [int(p["seed"]) for p in parts], "heldout_seeds": [int(p["seed"]) for p in hold]})
     m.save(args.out)
