@@ -98,3 +98,20 @@ def test_predictor_space_matches_the_library():
     lib = [(c.block, c.items, c.ctas_per_sm, c.schedule) for c in out]
     assert lib == learn.config_space()
     assert all(c.use_partition == 0 for c in out)
+
+
+def test_batched_queue_order_keeps_every_wait_behind_its_target(tmp_path):
+    """The batched kernel's work-queue order (both orders, several lags), compiled from its header
+    and checked on random list mixes: a permutation in which every item follows what it waits for."""
+    import os
+    import pytest
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cuda_inc = "/usr/local/cuda/include"
+    if not os.path.exists(os.path.join(cuda_inc, "vector_types.h")):
+        pytest.skip("CUDA headers not available")
+    exe = tmp_path / "order_check"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", os.path.join(root, "tests", "cpp", "order_check.cpp"), "-o", str(exe),
+                        "-I", os.path.join(root, "redzone_b200", "csrc"), "-I", cuda_inc], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
