@@ -414,6 +414,19 @@ def own_arm(args):
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e_steps)
     barrier()
+    # The same pipelined loop from C++ through the C-ABI (redzone_b200/_lib/rz_e2e, the program a
+    # caller of the reference's redzone_CPU would write): no interpreter between the calls.
+    e2e_cpp = None
+    drv = ROOT / "redzone_b200" / "_lib" / "rz_e2e"
+    if drv.exists() and world == 1:
+        try:
+            r = subprocess.run([str(drv), str(N_LOG2), str(K_LOG2), str(e_steps), str(E_DEPTH), str(E_SETS)],
+                               capture_output=True, text=True, timeout=600)
+            out = json.loads(r.stdout.strip().splitlines()[-1]) if r.stdout.strip() else {}
+            if r.returncode == 0 and "ms_per_step" in out:
+                e2e_cpp = out
+        except Exception:
+            e2e_cpp = None
     clk = clocks.stop()
     # The synchronous call, one step at a time (copy, kernel, read-back, host wait in series).
     s_ms = []
@@ -475,13 +488,13 @@ def own_arm(args):
             "floor_method": f"empty kernel of the removal's shape ({grid} x {block}, clusters of {cluster}) "
                             f"between the same events after the same scrub, {args.steps} steps",
             "removal_share_of_step": max(0.0, (mean_ms - floor_ms) / mean_ms),
-            "e2e": {"value": world * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 4 * k,
-                    "d2h_bytes_per_step": RESULT_BYTES, "ms_per_step": e2e_ms, "steps": e_steps,
-                    "method": f"rz_remove_host_idx_async, {E_DEPTH} calls in flight, each step's list copied from "
-                              f"pinned host memory and its status + length read back, rz_wait on every step; "
-                              f"time of the whole region / steps; {E_SETS} distinct lists, no L2 scrub",
-                    "serial_ms_per_step": e2e_serial_ms,
-                    "host_issue_us_per_call": 1e6 * issue_s / e_steps},
+            "e2e": e2e_line(k, world, e2e_cpp, {
+                "value": world * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 4 * k,
+                "d2h_bytes_per_step": RESULT_BYTES, "ms_per_step": e2e_ms, "steps": e_steps,
+                "method": f"Python (ctypes) caller: rz_remove_host_idx_async, {E_DEPTH} calls in flight, each "
+                          f"step's list copied from pinned host memory and its status + length read back, rz_wait "
+                          f"on every step; time of the whole region / steps; {E_SETS} distinct lists, no L2 scrub",
+                "serial_ms_per_step": e2e_serial_ms, "host_issue_us_per_call": 1e6 * issue_s / e_steps}),
             "cpu_baseline": cpu,
             "batched": bat,
             "clocks": clk,
@@ -491,6 +504,22 @@ def own_arm(args):
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def e2e_line(k: int, world: int, cpp: dict | None, py: dict) -> dict:
+    """The e2e object: the C++ caller's figure when its driver ran (the reference's users are C++
+    programs), else the Python caller's; both are kept."""
+    if cpp is None:
+        return dict(py, python=None)
+    return {"value": world * k / (cpp["ms_per_step"] * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": cpp["h2d_bytes_per_step"], "d2h_bytes_per_step": cpp["d2h_bytes_per_step"],
+            "ms_per_step": cpp["ms_per_step"], "steps": cpp["steps"],
+            "method": f"C++ caller through the C-ABI (redzone_b200/_lib/rz_e2e): rz_remove_host_idx_async, "
+                      f"{cpp['depth']} calls in flight, each step's list copied from pinned host memory and its "
+                      f"status + length read back, rz_wait on every step (status and length checked); CUDA events "
+                      f"around the whole region / steps; {cpp['sets']} distinct lists, no L2 scrub",
+            "serial_ms_per_step": cpp["serial_ms_per_step"], "host_issue_us_per_call": cpp["host_issue_us_per_call"],
+            "python": py}
 
 
 # ------------------------------------------------------------------------------------------------

@@ -19,6 +19,7 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 OBJ_DIR = PKG / "_lib" / "obj"
 LIB = OUT_DIR / "libredzone_b200.so"
+E2E = OUT_DIR / "rz_e2e"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -65,6 +66,7 @@ def build(verbose: bool = False, quiet: bool = False) -> Path:
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
         if not quiet:
             print(f"redzone_b200: {LIB.name} up to date ({len(srcs)} sources, none rebuilt)")
+        build_e2e_driver(quiet)
         return LIB
     cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcuda"]
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -73,7 +75,26 @@ def build(verbose: bool = False, quiet: bool = False) -> Path:
     if not quiet:
         print(f"redzone_b200: rebuilt {len(rebuilt)} of {len(srcs)} sources "
               f"({', '.join(rebuilt) if rebuilt else 'objects newer than the library'}); linked {LIB.name}")
+    build_e2e_driver(quiet)
     return LIB
+
+
+def build_e2e_driver(quiet: bool = False) -> Path:
+    """The C++ end-to-end timing program (redzone_b200/e2e_driver.cpp), linked against the library
+    it sits next to."""
+    src = PKG / "e2e_driver.cpp"
+    if E2E.exists() and E2E.stat().st_mtime >= max(src.stat().st_mtime, LIB.stat().st_mtime,
+                                                    (ROOT / "include" / "redzone.h").stat().st_mtime):
+        return E2E
+    cuda = Path(NVCC).resolve().parent.parent
+    cmd = ["g++", "-std=c++17", "-O2", str(src), "-o", str(E2E), f"-I{ROOT / 'include'}", f"-I{cuda / 'include'}",
+           f"-L{OUT_DIR}", "-lredzone_b200", "-Wl,-rpath,$ORIGIN", f"-L{cuda / 'lib64'}", "-lcudart"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"e2e driver build failed:\n{res.stdout}\n{res.stderr}")
+    if not quiet:
+        print(f"redzone_b200: built {E2E.name}")
+    return E2E
 
 
 if __name__ == "__main__":

@@ -115,3 +115,12 @@ def test_batched_queue_order_keeps_every_wait_behind_its_target(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def test_e2e_driver_is_built_and_checks_its_arguments():
+    """build() also links the C++ end-to-end timing program next to the library; with bad
+    arguments it reports the error before touching a GPU."""
+    exe = _native.LIB_PATH.parent / "rz_e2e"
+    assert exe.exists()
+    r = subprocess.run([str(exe), "10", "10", "5", "4"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and '"error": "bad arguments"' in r.stdout
