@@ -88,7 +88,8 @@ def build_e2e_driver(quiet: bool = False) -> Path:
         return E2E
     cuda = Path(NVCC).resolve().parent.parent
     cmd = ["g++", "-std=c++17", "-O2", str(src), "-o", str(E2E), f"-I{ROOT / 'include'}", f"-I{cuda / 'include'}",
-           f"-L{OUT_DIR}", "-lredzone_b200", "-Wl,-rpath,$ORIGIN", f"-L{cuda / 'lib64'}", "-lcudart"]
+           f"-L{OUT_DIR}", "-lredzone_b200", "-Wl,-rpath,$ORIGIN", f"-L{cuda / 'lib64'}", "-lcudart_static",
+           "-ldl", "-lpthread", "-lrt"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"e2e driver build failed:\n{res.stdout}\n{res.stderr}")
