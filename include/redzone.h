@@ -127,13 +127,13 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
  * Pipelined form of rz_remove_host_idx for a host program that hands the GPU one removal list
  * after another (redzone_CPU, Redzone_CPU.hxx:150, called in a loop): returns without waiting.
  * The index list is copied on the context's own copy stream, so the copy of one call overlaps
- * the kernel of the one before; the removal runs on `stream` after its copy, followed by a short
- * read-back of the call's status and device-tracked length into pinned memory. *ticket names the
- * call for rz_wait. h_idx (ideally pinned) must stay unchanged until rz_wait for the call returns.
- * Calls are ordered on `stream` as issued. Up to 4 calls per context are in flight; issuing a 5th
- * waits for the oldest (its result is kept for rz_wait). The staging buffers grow to the largest
- * k seen (context scratch). After a device error the status is sticky on the device until the
- * wait that reads it, so calls issued in between report it too.
+ * the kernel of the one before; the removal runs on `stream` after its copy; the call's own
+ * status and device-tracked length are read back into pinned memory on a third stream while the
+ * next removal runs. *ticket names the call for rz_wait. h_idx (ideally pinned) must stay
+ * unchanged until rz_wait for the call returns. Calls are ordered on `stream` as issued. Up to 4
+ * calls per context are in flight; issuing a 5th waits for the oldest (its result is kept for
+ * rz_wait). The staging buffers grow to the largest k seen (context scratch). Each call reports
+ * only its own device errors.
  */
 int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes,
                              const uint32_t* h_idx, int64_t k, uint32_t flags, rz_stream_t stream,

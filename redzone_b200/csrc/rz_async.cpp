@@ -4,14 +4,15 @@
 // waits, so consecutive calls run strictly one after another: copy, kernel, read-back, host
 // wake-up. A host program that feeds the GPU a stream of removal lists (the reference's
 // redzone_CPU call shape, Redzone_CPU.hxx:150, called in a loop) can instead issue calls without
-// waiting and collect each result later. Per context there is a ring of kSlots staging slots,
-// each with a device copy of one index list, a pinned copy of the call's status and device
-// length, and two events:
-//   copy stream : H2D  h_idx -> slot.d_idx ; record slot.copied
-//   call stream : wait slot.copied ; removal kernel(s) ; D2H status|length -> slot.h_res ;
-//                 record slot.done
-// The index copy of call i+1 runs on the copy stream while call i's kernel runs, so a caller that
-// keeps a few calls in flight pays for the kernels and the short read-backs, not for the copies.
+// waiting and collect each result later. Per context there is a ring of kSlots slots, each with a
+// device copy of one index list, its own device status word and length word (the call's kernels
+// write those instead of the context's, so calls in flight never share them), a pinned copy of
+// both, and three events. Three streams:
+//   copy stream : zero slot.status ; H2D h_idx -> slot.d_idx ; record slot.copied
+//   call stream : wait slot.copied ; removal kernel(s) ; record slot.kdone
+//   read stream : wait slot.kdone ; D2H slot.status|length -> slot.h_res ; record slot.done
+// The index copy of call i+1 runs while call i's kernel runs, and call i's read-back while call
+// i+1's kernel runs, so with a few calls in flight the call stream runs the kernels back to back.
 // A slot is reused only after its previous call was collected (rz_wait) or, when the caller
 // issues more than kSlots calls ahead, after the issuing call has waited for it and kept its
 // result for a later rz_wait.
@@ -28,12 +29,15 @@ namespace {
 
 constexpr int kSlots = 4;
 constexpr size_t kStashMax = 1024;  // results of calls evicted from their slot before rz_wait
+constexpr size_t kSlotResBytes = 1024;  // a slot's device status (offset 0) and length (offset 512)
 
 struct Slot {
     uint32_t* d_idx = nullptr;
     size_t cap = 0;                  // entries of d_idx
-    uint8_t* h_res = nullptr;        // pinned: status word at 0, device length at 512
+    uint8_t* d_res = nullptr;        // device: status word at 0, device length at 512
+    uint8_t* h_res = nullptr;        // pinned copy of the same kResultBytes
     cudaEvent_t copied = nullptr;
+    cudaEvent_t kdone = nullptr;
     cudaEvent_t done = nullptr;
     uint64_t ticket = 0;
     int64_t k = 0, n = 0;
@@ -50,6 +54,8 @@ struct Result {
 
 struct AsyncPipe {
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t read_stream = nullptr;
+    uint8_t* d_res = nullptr;        // kSlots * kSlotResBytes
     Slot slots[kSlots];
     std::deque<Result> stash;
     uint64_t next_ticket = 1;
@@ -57,28 +63,41 @@ struct AsyncPipe {
 
 namespace {
 
+void pipe_free(AsyncPipe* p) {
+    for (Slot& s : p->slots) {
+        cudaFree(s.d_idx);
+        if (s.h_res) cudaFreeHost(s.h_res);
+        if (s.copied) cudaEventDestroy(s.copied);
+        if (s.kdone) cudaEventDestroy(s.kdone);
+        if (s.done) cudaEventDestroy(s.done);
+    }
+    cudaFree(p->d_res);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+    if (p->read_stream) cudaStreamDestroy(p->read_stream);
+    delete p;
+}
+
 int pipe_create(rz_ctx* ctx, AsyncPipe** out) {
     AsyncPipe* p = new (std::nothrow) AsyncPipe();
     if (!p) return RZ_ERR_NO_MEMORY;
     cudaError_t e = cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->read_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_res, kSlots * kSlotResBytes);
+    if (e == cudaSuccess) e = cudaMemset(p->d_res, 0, kSlots * kSlotResBytes);
     for (int i = 0; i < kSlots && e == cudaSuccess; ++i) {
         Slot& s = p->slots[i];
+        s.d_res = p->d_res + size_t(i) * kSlotResBytes;
         void* h = nullptr;
         e = cudaMallocHost(&h, kResultBytes);
         if (e != cudaSuccess) break;
         s.h_res = static_cast<uint8_t*>(h);
         e = cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.kdone, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
     }
     if (e != cudaSuccess) {
         const int st = cuda_fail(ctx, e, "asynchronous pipeline");
-        for (Slot& s : p->slots) {
-            if (s.h_res) cudaFreeHost(s.h_res);
-            if (s.copied) cudaEventDestroy(s.copied);
-            if (s.done) cudaEventDestroy(s.done);
-        }
-        if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
-        delete p;
+        pipe_free(p);
         return st;
     }
     *out = p;
@@ -86,7 +105,7 @@ int pipe_create(rz_ctx* ctx, AsyncPipe** out) {
 }
 
 // The finished call of a pending slot: its status (mapped) and device-tracked length. A device
-// error marks the context scratch for a reset before its next call and clears the status word.
+// error marks the context scratch for a reset before its next call.
 int collect(rz_ctx* ctx, Slot& s, Result* r) {
     const int st = wait_event(ctx, s.done);
     if (st != RZ_OK) return st;
@@ -95,15 +114,28 @@ int collect(rz_ctx* ctx, Slot& s, Result* r) {
     std::memcpy(&bits, s.h_res, sizeof(bits));
     std::memcpy(&len, s.h_res + 512, sizeof(len));
     s.pending = false;
-    if (bits) {
-        RZ_CUDA_TRY(ctx, cudaMemset(ctx->ws.status, 0, sizeof(uint32_t)));
-        ctx->ws.dirty = true;
-    }
+    if (bits) ctx->ws.dirty = true;
     r->ticket = s.ticket;
     r->status = map_status(bits);
     r->new_len = (s.k > 0 && s.k < s.n) ? int64_t(len) : s.n - s.k;
     return RZ_OK;
 }
+
+// Aim the context's status and length words at a slot's for the duration of one launch: every
+// kernel takes both pointers from the context when it is launched.
+struct ResultRedirect {
+    rz_ctx* ctx;
+    uint32_t* status;
+    unsigned long long* dev_len;
+    ResultRedirect(rz_ctx* c, uint8_t* d_res) : ctx(c), status(c->ws.status), dev_len(c->ws.dev_len) {
+        ctx->ws.status = reinterpret_cast<uint32_t*>(d_res);
+        ctx->ws.dev_len = reinterpret_cast<unsigned long long*>(d_res + 512);
+    }
+    ~ResultRedirect() {
+        ctx->ws.status = status;
+        ctx->ws.dev_len = dev_len;
+    }
+};
 
 }  // namespace
 
@@ -111,15 +143,10 @@ void release_async(rz_ctx* ctx) {
     AsyncPipe* p = static_cast<AsyncPipe*>(ctx->async_pipe);
     if (!p) return;
     cudaStreamSynchronize(p->copy_stream);
-    for (Slot& s : p->slots) {
+    cudaStreamSynchronize(p->read_stream);
+    for (Slot& s : p->slots)
         if (s.done) cudaEventSynchronize(s.done);
-        cudaFree(s.d_idx);
-        if (s.h_res) cudaFreeHost(s.h_res);
-        if (s.copied) cudaEventDestroy(s.copied);
-        if (s.done) cudaEventDestroy(s.done);
-    }
-    cudaStreamDestroy(p->copy_stream);
-    delete p;
+    pipe_free(p);
     ctx->async_pipe = nullptr;
 }
 
@@ -174,15 +201,24 @@ int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem
         ctx->scratch_held += want * 4;
     }
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
-    if (k > 0) {
+    // Copy stream: the slot's status word starts at zero, then the index list arrives.
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(s.d_res, 0, sizeof(uint32_t), P.copy_stream));
+    if (k > 0)
         RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.d_idx, h_idx, size_t(k) * 4, cudaMemcpyHostToDevice, P.copy_stream));
-        RZ_CUDA_TRY(ctx, cudaEventRecord(s.copied, P.copy_stream));
-        RZ_CUDA_TRY(ctx, cudaStreamWaitEvent(cs, s.copied, 0));
+    RZ_CUDA_TRY(ctx, cudaEventRecord(s.copied, P.copy_stream));
+    // Call stream: the removal, writing the slot's status and length words.
+    RZ_CUDA_TRY(ctx, cudaStreamWaitEvent(cs, s.copied, 0));
+    int st;
+    {
+        ResultRedirect redirect(ctx, s.d_res);
+        st = rz_remove(ctx, d_data, n, elem_bytes, s.d_idx, k, nullptr, flags & ~uint32_t(RZ_SYNC), stream);
     }
-    const int st = rz_remove(ctx, d_data, n, elem_bytes, s.d_idx, k, nullptr, flags & ~uint32_t(RZ_SYNC), stream);
     if (st != RZ_OK) return st;
-    RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.h_res, ctx->ws.status, kResultBytes, cudaMemcpyDeviceToHost, cs));
-    RZ_CUDA_TRY(ctx, cudaEventRecord(s.done, cs));
+    RZ_CUDA_TRY(ctx, cudaEventRecord(s.kdone, cs));
+    // Read stream: the result comes back while the call stream runs the next removal.
+    RZ_CUDA_TRY(ctx, cudaStreamWaitEvent(P.read_stream, s.kdone, 0));
+    RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.h_res, s.d_res, kResultBytes, cudaMemcpyDeviceToHost, P.read_stream));
+    RZ_CUDA_TRY(ctx, cudaEventRecord(s.done, P.read_stream));
     s.ticket = t;
     s.k = k;
     s.n = n;

@@ -96,3 +96,32 @@ def test_async_interleaved_waits_and_errors(ctx):
     exp = np.arange(n, dtype=np.int32)
     oracle.remove(exp, idx[1].astype(np.uint32))
     assert np.array_equal(b[: n - 4096].cpu().numpy(), exp[: n - 4096])
+
+
+def test_async_errors_stay_with_their_call(ctx):
+    """Each call has its own status word: a call rejected on the device (a repeated index under
+    RZ_VALIDATE) reports it, and the calls issued around it, still in flight, report success and
+    give the canonical result."""
+    n, k = 1 << 18, 4096
+    good = [workloads.uniform(n, k, seed=70 + s).astype(np.int32) for s in range(3)]
+    bad = good[0].copy()
+    bad[5] = bad[6]
+    arrays = [torch.arange(n, dtype=torch.int32, device=DEV) for _ in range(4)]
+    lists = [good[0], bad, good[1], good[2]]
+    pinned = [torch.from_numpy(x).pin_memory() for x in lists]
+    tickets = [ctx.remove_host_idx_async(arrays[0], pinned[0]),
+               ctx.remove_host_idx_async(arrays[1], pinned[1], flags=rz.RZ_VALIDATE),
+               ctx.remove_host_idx_async(arrays[2], pinned[2]),
+               ctx.remove_host_idx_async(arrays[3], pinned[3])]
+    results = []
+    for t in tickets:
+        try:
+            results.append(ctx.wait(t))
+        except rz.RedzoneError as e:
+            results.append(-e.code)
+    assert results == [n - k, -_native.RZ_ERR_DUPLICATE, n - k, n - k]
+    assert torch.equal(arrays[1], torch.arange(n, dtype=torch.int32, device=DEV))  # rejected: untouched
+    for j in (0, 2, 3):
+        exp = np.arange(n, dtype=np.int32)
+        oracle.remove(exp, lists[j].astype(np.uint32))
+        assert np.array_equal(arrays[j][: n - k].cpu().numpy(), exp[: n - k])
