@@ -8,9 +8,11 @@
 // device copy of one index list, its own device status word and length word (the call's kernels
 // write those instead of the context's, so calls in flight never share them), a pinned copy of
 // both, and three events. Three streams:
-//   copy stream : zero slot.status ; H2D h_idx -> slot.d_idx ; record slot.copied
+//   copy stream : H2D h_idx -> slot.d_idx ; record slot.copied
 //   call stream : wait slot.copied ; removal kernel(s) ; record slot.kdone
-//   read stream : wait slot.kdone ; D2H slot.status|length -> slot.h_res ; record slot.done
+//   read stream : wait slot.kdone ; D2H slot.status|length -> slot.h_res ; zero slot.status ;
+//                 record slot.done
+// (A slot is reused only after the host has seen its `done`, so its status word is zero again.)
 // The index copy of call i+1 runs while call i's kernel runs, and call i's read-back while call
 // i+1's kernel runs, so with a few calls in flight the call stream runs the kernels back to back.
 // A slot is reused only after its previous call was collected (rz_wait) or, when the caller
@@ -201,8 +203,8 @@ int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem
         ctx->scratch_held += want * 4;
     }
     cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
-    // Copy stream: the slot's status word starts at zero, then the index list arrives.
-    RZ_CUDA_TRY(ctx, cudaMemsetAsync(s.d_res, 0, sizeof(uint32_t), P.copy_stream));
+    // Copy stream: the index list arrives (the slot's status word is zero: it starts so, and the
+    // read stream clears it after each read-back, before the slot's `done`).
     if (k > 0)
         RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.d_idx, h_idx, size_t(k) * 4, cudaMemcpyHostToDevice, P.copy_stream));
     RZ_CUDA_TRY(ctx, cudaEventRecord(s.copied, P.copy_stream));
@@ -218,6 +220,7 @@ int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem
     // Read stream: the result comes back while the call stream runs the next removal.
     RZ_CUDA_TRY(ctx, cudaStreamWaitEvent(P.read_stream, s.kdone, 0));
     RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.h_res, s.d_res, kResultBytes, cudaMemcpyDeviceToHost, P.read_stream));
+    RZ_CUDA_TRY(ctx, cudaMemsetAsync(s.d_res, 0, sizeof(uint32_t), P.read_stream));
     RZ_CUDA_TRY(ctx, cudaEventRecord(s.done, P.read_stream));
     s.ticket = t;
     s.k = k;
