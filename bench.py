@@ -387,10 +387,10 @@ def own_arm(args):
 
     # ---- end to end through the public C-ABI with host buffers: every step copies its removal
     # list from pinned host memory and reads its result (status + device-tracked length) back.
-    # Pipelined: rz_remove_host_idx_async keeps up to E_DEPTH calls in flight, so the copy of
+    # Pipelined: rz_remove_host_idx_async keeps E_DEPTH calls in flight, so the copy of
     # step i+1 overlaps the kernel of step i; each step is collected with rz_wait. No L2 scrub
     # inside this region (each step's list arrives fresh over PCIe; E_SETS distinct lists) ----
-    E_SETS, E_DEPTH = 64, 4
+    E_SETS, E_DEPTH = 64, 6
     e_np = [workloads.uniform(n, k, seed=dist.replica_seed(1000 + s, rank)) for s in range(E_SETS)]
     e_pinned = [torch.from_numpy(s.astype(np.int32)).pin_memory() for s in e_np]
     for i in range(max(args.warmup, E_DEPTH + 1)):  # first use grows the staging slots

@@ -130,8 +130,8 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
  * the kernel of the one before; the removal runs on `stream` after its copy; the call's own
  * status and device-tracked length are read back into pinned memory on a third stream while the
  * next removal runs. *ticket names the call for rz_wait. h_idx (ideally pinned) must stay
- * unchanged until rz_wait for the call returns. Calls are ordered on `stream` as issued. Up to 4
- * calls per context are in flight; issuing a 5th waits for the oldest (its result is kept for
+ * unchanged until rz_wait for the call returns. Calls are ordered on `stream` as issued. Up to 8
+ * calls per context are in flight; issuing a 9th waits for the oldest (its result is kept for
  * rz_wait). The staging buffers grow to the largest k seen (context scratch). Each call reports
  * only its own device errors.
  */

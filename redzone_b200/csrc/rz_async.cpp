@@ -29,7 +29,7 @@ namespace rz {
 
 namespace {
 
-constexpr int kSlots = 4;
+constexpr int kSlots = 8;
 constexpr size_t kStashMax = 1024;  // results of calls evicted from their slot before rz_wait
 constexpr size_t kSlotResBytes = 1024;  // a slot's device status (offset 0) and length (offset 512)
 
