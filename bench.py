@@ -4,22 +4,33 @@
 Workload (the large-list configuration the headline target is quoted on): n = 2^28 int32 items
 (iota), k = 2^16 distinct removal indices drawn uniformly without replacement, unsorted. A step
 is one Redzone removal of k items from the device-resident list. L2 is flushed between timed
-steps (a 256 MiB scrub write), and the removal lists rotate over 8 seeds.
+steps (a 256 MiB scrub write, one before the first step too), and the removal lists rotate over
+8 seeds.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl own|reference] [--sweep]
 
 Own arm: CUDA-event time of each rz_remove kernel on the launching stream; value = k / mean
 step time (whole job: summed over ranks; N > 1 runs independent replicas, max over ranks).
-Also reported: roofline of the Redzone kernel against measured HBM bandwidth, the O(n)
-partition comparator on the same workload, an end-to-end figure through rz_remove_host_idx
-(removal list copied from pinned host memory, new length read back, every step), the
-reference's own CPU Redzone timed on this host, and SM clocks sampled during the timed region.
+Also reported on the same line:
+  * the event floor (an empty kernel of the removal's launch shape, timed the same way);
+  * the roofline of the Redzone kernel against measured HBM bandwidth;
+  * the O(n) partition comparator and the reference's own mark + thrust::remove comparator on the
+    same workload, and a CUDA-graph steady state of the removal;
+  * end to end (e2e): the pipelined host-index call (rz_remove_host_idx_async / rz_wait) from C++
+    (redzone_b200/_lib/rz_e2e) and from Python, each step copying its removal list from pinned
+    host memory and reading its status and length back;
+  * the batched half of the metric: 4096 uneven lists in one launch with the configuration the
+    learned list-mix predictor picks, against per-list launches, the default configuration, an
+    exhaustive autotune of the configuration space, and the hole writes alone;
+  * the reference's CPU paths on the host cores (redzone_CPU, and std::remove(par_unseq));
+  * SM clocks sampled from before the timed region to the end of the e2e leg.
 
-Other workloads: --workload batched (4096 lists, one launch), --workload service (streaming
+Other workloads: --workload batched (the batched leg alone), --workload service (streaming
 deletes), --workload produced (a list made on the GPU with fused red-zone marking), --sweep (k).
 
 Reference arm (--impl reference): the reference's redzone_CPU (compiled from its sources into
-oracle/_ref) on the same workload on the host cores, rank 0 only.
+oracle/_ref) on the same workload on the host cores, rank 0 only, with std::remove(par_unseq)
+beside it; it loads no library of this package.
 """
 from __future__ import annotations
 
