@@ -131,7 +131,7 @@ int main(int argc, char** argv) {
     cudaEventElapsedTime(&sync_ms, e0, e1);
 
     std::printf("{\"ms_per_step\": %.6f, \"steps\": %d, \"depth\": %d, \"sets\": %d, \"host_issue_us_per_call\": %.3f, "
-                "\"serial_ms_per_step\": %.6f, \"h2d_bytes_per_step\": %lld, \"d2h_bytes_per_step\": 520}\n",
+                "\"serial_ms_per_step\": %.6f, \"h2d_bytes_per_step\": %lld, \"d2h_bytes_per_step\": 16}\n",
                 pipelined_ms / steps, steps, depth, sets, 1e6 * issue_s / steps, sync_ms / sync_steps,
                 (long long)(k * 4));
     rz_destroy(ctx);

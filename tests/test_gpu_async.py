@@ -125,3 +125,35 @@ def test_async_errors_stay_with_their_call(ctx):
         exp = np.arange(n, dtype=np.int32)
         oracle.remove(exp, lists[j].astype(np.uint32))
         assert np.array_equal(arrays[j][: n - k].cpu().numpy(), exp[: n - k])
+
+
+@pytest.mark.parametrize("k", [1 << 10, 1 << 14, 1 << 18])
+def test_async_error_reports_and_slot_reuse(ctx, k):
+    """An out-of-range index in one call comes back from that call's rz_wait, whichever kernel ran
+    (scan-all at 2^10, cluster scan at 2^14 -- both hand their result over from the kernel -- and
+    the grid schedule at 2^18, which uses the read-back copy), and the calls issued after it on
+    the same staging slots report success with the canonical result: the slot's status word
+    starts clean again."""
+    n = 1 << 21
+    calls = 20
+    lists = [workloads.uniform(n, k, seed=500 + j).astype(np.int64) for j in range(calls)]
+    bad_at = 3
+    lists[bad_at][k // 2] = n + 5
+    pinned = [torch.from_numpy(x.astype(np.uint32).view(np.int32)).pin_memory() for x in lists]
+    arrays = [torch.arange(n, dtype=torch.int32, device=DEV) for _ in range(calls)]
+    tickets = [ctx.remove_host_idx_async(a, x) for a, x in zip(arrays, pinned)]
+    for j, t in enumerate(tickets):
+        if j == bad_at:
+            with pytest.raises(rz.RedzoneError) as e:
+                ctx.wait(t)
+            assert e.value.code == _native.RZ_ERR_OUT_OF_RANGE
+        else:
+            assert ctx.wait(t) == n - k
+    for j in (0, bad_at + 1, bad_at + 8, calls - 1):
+        exp = np.arange(n, dtype=np.int32)
+        oracle.remove(exp, lists[j].astype(np.uint32))
+        assert np.array_equal(arrays[j][: n - k].cpu().numpy(), exp[: n - k]), j
+    # The same slots once more, one call at a time: every status word is zero.
+    for j in range(10):
+        b = torch.arange(n, dtype=torch.int32, device=DEV)
+        assert ctx.wait(ctx.remove_host_idx_async(b, pinned[(j + 4) % calls])) == n - k
