@@ -116,8 +116,15 @@ __device__ __forceinline__ void write_orphans(const bool* dv, const bool* sv, co
     (void)lane;
 }
 
+// Two 512-thread CTAs per SM (at most 64 registers) where one thread's items take at most 64
+// bytes: measured on the 4096-list workload, the doubled resident warps keep more random hole
+// writes in flight (best configuration 12.73 -> 10.17 ms). Wider variants would spill at 64
+// registers (144-644 bytes) and keep the compiler's choice (up to 128).
 template <int W, int IPT>
-__global__ void redzone_batched_kernel(const BatchParams p) {
+constexpr int batched_min_blocks() { return W * IPT <= 64 ? 2 : 1; }
+
+template <int W, int IPT>
+__global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_batched_kernel(const BatchParams p) {
     using T = typename Payload<W>::T;
     const int B = blockDim.x, lane = threadIdx.x & 31;
     const uint32_t TILE = uint32_t(B) * IPT;
