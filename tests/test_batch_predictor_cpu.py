@@ -33,8 +33,9 @@ def test_batch_config_space():
     assert {i for _, i, _, _ in space} == {2, 4, 8}
     assert {c for _, _, c, _ in space} == {1, 2, 4}
     assert {wv for _, _, _, wv in space} == {0, learn_batched.DEFAULT_WAVE}
-    for w in (4, 8, 16, 32):
-        assert space[learn_batched.default_class(None, w)][0] == 256
+    for w in (4, 8, 16):
+        assert space[learn_batched.default_class(None, w)] == (512, 4, 4, learn_batched.DEFAULT_WAVE)
+    assert space[learn_batched.default_class(None, 32)] == (256, 8, 4, 0)
 
 
 def test_soft_targets_ignore_infeasible_configurations():
