@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
     __shared__ uint32_t s_pfx[2 * kMaxTilesPerList + 2];  // PAIR: per-tile prefixes of D and S
     __shared__ uint32_t s_scan[33];
 
+    const uint64_t pol_stream = l2_policy_evict_first(), pol_hole = l2_policy_evict_last();
     // The next ticket is taken one item ahead, so its atomic overlaps the current item's work.
     uint32_t next_t = 0;
     if (threadIdx.x == 0) next_t = atomicAdd(&p.counters[0], 1u);
@@ -203,8 +204,8 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
                 const uint32_t i = uint32_t(j) * B + threadIdx.x;
                 rr[j] = 0xffffffffu;
                 if (i < k) {
-                    rr[j] = __ldg(&L.idx[i]);
-                    src[j] = tail[i];  // loaded with the index, needed or not: one round trip
+                    rr[j] = ld_hint(&L.idx[i], pol_stream);
+                    src[j] = ld_hint(tail + i, pol_stream);  // loaded with the index, needed or not: one round trip
                 }
             }
             for (uint32_t w = threadIdx.x; w < TILE / 32; w += B) s_bits[w] = 0u;
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
             }
 #pragma unroll
             for (int j = 0; j < IPT; ++j)
-                if (dv[j] && sv[j]) head[rr[j]] = src[j];
+                if (dv[j] && sv[j]) st_hint(head + rr[j], src[j], pol_hole);
             const uint32_t tot = rank_orphans<IPT>(dv, sv, dmask, smask, s_cnt);
             if (tot != 0u) {
                 write_orphans<IPT>(dv, sv, dmask, smask, rr, s_cnt, 0, cut, s_dl, s_sl);
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
                 const uint32_t dcnt = tot >> 16, scnt = tot & 0xffffu;
                 const uint32_t m = min(dcnt, scnt);
                 for (uint32_t r = threadIdx.x; r < m; r += B)
-                    head[s_dl[r]] = reinterpret_cast<const T*>(L.data)[s_sl[r]];
+                    st_hint(head + s_dl[r], reinterpret_cast<const T*>(L.data)[s_sl[r]], pol_hole);
                 if (dcnt > scnt && threadIdx.x == 0) atomicOr(p.status, ST_INCONSISTENT);
             }
             continue;
@@ -267,9 +268,9 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
                 for (int j = 0; j < IPT; ++j) {
                     const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
                     if (i < k) {
-                        rr[j] = __ldg(&L.idx[i]);
+                        rr[j] = ld_hint(&L.idx[i], pol_stream);
                         word[j] = __ldcg(&p.bitmap[L.bitmap_off + (i >> 5)]);
-                        src[j] = tail[i];
+                        src[j] = ld_hint(tail + i, pol_stream);
                     } else {
                         rr[j] = 0xffffffffu;
                         word[j] = 0u;
@@ -287,7 +288,7 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
                 }
 #pragma unroll
                 for (int j = 0; j < IPT; ++j)
-                    if (dv[j] && sv[j]) head[rr[j]] = src[j];
+                    if (dv[j] && sv[j]) st_hint(head + rr[j], src[j], pol_hole);
                 __syncwarp();  // every lane has read its bitmap word before lane 0 clears it
                 if (lane == 0) {
 #pragma unroll
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
                 const int c2 = owner_of_rank(pfx_s, int(nch), jr);
                 const uint32_t pos = __ldcg(&p.slist[L.list_off + uint64_t(c2) * TILE + (jr - pfx_s[c2])]);
                 const uint32_t dest = __ldcg(&p.dlist[L.list_off + uint64_t(c) * TILE + r]);
-                head[dest] = reinterpret_cast<const T*>(L.data)[pos];
+                st_hint(head + dest, reinterpret_cast<const T*>(L.data)[pos], pol_hole);
             }
         }
     }

@@ -61,6 +61,57 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// ---- L2 eviction priorities (createpolicy + L2::cache_hint) ----------------------------------
+// Read-once streams (a list's index entries and tail items on their last read) go in as
+// evict-first, hole stores as evict-last: partially written hole lines then stay in L2 while
+// more writes to the same sectors may arrive, instead of being pushed out by the stream.
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint32_t ld_hint(const uint32_t* a, uint64_t pol) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ uint2 ld_hint(const uint2* a, uint64_t pol) {
+    uint2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.b32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ uint4 ld_hint(const uint4* a, uint64_t pol) {
+    uint4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.b32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ u32x8 ld_hint(const u32x8* a, uint64_t pol) {
+    u32x8 v;
+    v.a = ld_hint(&a->a, pol);
+    v.b = ld_hint(&a->b, pol);
+    return v;
+}
+__device__ __forceinline__ void st_hint(uint32_t* a, uint32_t v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(uint2* a, uint2 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v2.b32 [%0], {%1, %2}, %3;" ::"l"(a), "r"(v.x), "r"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(uint4* a, uint4 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v4.b32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "r"(v.x), "r"(v.y),
+                 "r"(v.z), "r"(v.w), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(u32x8* a, const u32x8& v, uint64_t pol) {
+    st_hint(&a->a, v.a, pol);
+    st_hint(&a->b, v.b, pol);
+}
+
 // ---- result hand-off of a pipelined host-index call (PublishArgs) ----------------------------
 // publish_length: thread 0 of CTA 0 writes {ticket, new length} into the result words with one
 // 16-byte store at the start of the kernel, where the PCIe write has long completed by the time
