@@ -661,8 +661,8 @@ def batched_leg(args, ctx, dev, world: int, rank: int, steps: int, warmup: int) 
     payload = list id << 32 | index) in one persistent graph-replayed launch, its configuration
     picked by the learned list-mix predictor, against one rz_remove launch per list (stream-
     launched, and the same launches captured in one CUDA graph), against the built-in default
-    configuration, and against every configuration of the space (exhaustive autotune: the judge
-    of the predictor's regret). N > 1: the lists are partitioned across ranks by removals
+    configuration, and against every configuration of the space (exhaustive autotune: the
+    reference point of the predictor's regret). N > 1: the lists are partitioned across ranks by removals
     (contiguous, balanced), each rank runs its share as one launch; no collective on the data path,
     max-over-ranks timing. The payload (about 14 GB) is far larger than L2."""
     import torch

@@ -11,7 +11,7 @@ Pipeline (``python -m redzone_b200.learn collect|train``; ``train`` also evaluat
 * ``train``: soft targets (configurations within a few percent of the fastest get most of the
   mass) and the partition bit; Adam on the GPU through ``rz_mlp_train``.
 * evaluation (end of ``train``): on held-out seeds, regret = time of the predicted
-  configuration / time of the best one - 1 (the exhaustive autotune table is the judge);
+  configuration / time of the best one - 1 (the best one taken from the exhaustive autotune table);
   compared with the fixed default configuration (``rz_default_cfg``), i.e. the method without
   the network.
 
