@@ -157,3 +157,25 @@ def test_async_error_reports_and_slot_reuse(ctx, k):
     for j in range(10):
         b = torch.arange(n, dtype=torch.int32, device=DEV)
         assert ctx.wait(ctx.remove_host_idx_async(b, pinned[(j + 4) % calls])) == n - k
+
+
+@pytest.mark.parametrize("k", [1 << 10, 1 << 14])
+def test_async_validation_abort_reports_duplicate(ctx, k):
+    """A repeated index under RZ_VALIDATE stops the removal kernel before it moves anything
+    (scan-all at 2^10, cluster scan at 2^14: both report from the kernel's abort path), rz_wait
+    returns RZ_ERR_DUPLICATE, the array is untouched, and the next call on the context succeeds."""
+    n = 1 << 20
+    good = workloads.uniform(n, k, seed=90 + k).astype(np.int32)
+    bad = good.copy()
+    bad[k // 2] = bad[k // 2 + 1]
+    a = torch.arange(n, dtype=torch.int32, device=DEV)
+    t = ctx.remove_host_idx_async(a, torch.from_numpy(bad).pin_memory(), flags=rz.RZ_VALIDATE)
+    with pytest.raises(rz.RedzoneError) as e:
+        ctx.wait(t)
+    assert e.value.code == _native.RZ_ERR_DUPLICATE
+    assert torch.equal(a, torch.arange(n, dtype=torch.int32, device=DEV))
+    t = ctx.remove_host_idx_async(a, torch.from_numpy(good).pin_memory(), flags=rz.RZ_VALIDATE)
+    assert ctx.wait(t) == n - k
+    exp = np.arange(n, dtype=np.int32)
+    oracle.remove(exp, good.astype(np.uint32))
+    assert np.array_equal(a[: n - k].cpu().numpy(), exp[: n - k])
