@@ -287,6 +287,8 @@ int rz_default_cfg(const rz_ctx* ctx, int64_t n, int64_t k, uint32_t elem_bytes,
 
 /* ---- many lists in one launch --------------------------------------------------------------- */
 /* One list: device pointers to its payload (n items) and its k distinct removal indices. */
+/* One list of a batch: data aligned to min(elem_bytes, 16) bytes, idx to 4 bytes
+ * (RZ_ERR_INVALID_ARG otherwise). */
 typedef struct rz_list_desc {
     void* data;
     const uint32_t* idx;

@@ -406,6 +406,13 @@ struct rz_batch_plan {
 
 namespace rz {
 
+// Items are read and written as whole w-byte units (16-byte vectors for w >= 16) and index
+// entries as 4-byte words: both must be aligned to them.
+static bool list_aligned(const rz_list_desc& d, uint32_t w) {
+    const uintptr_t a = w >= 16 ? 16 : w;
+    return (reinterpret_cast<uintptr_t>(d.data) % a) == 0 && (reinterpret_cast<uintptr_t>(d.idx) % 4) == 0;
+}
+
 static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, uint32_t w, const rz_batch_cfg& cfg_in,
                       rz_batch_plan* plan) {
     rz_batch_cfg cfg = cfg_in;
@@ -436,6 +443,7 @@ static int plan_build(rz_ctx* ctx, const rz_list_desc* lists, int32_t nlists, ui
         const rz_list_desc& d = lists[l];
         if (d.n < 0 || d.k < 0 || d.k > d.n || d.n >= (int64_t(1) << 32)) return RZ_ERR_INVALID_ARG;
         if (d.k > 0 && (!d.data || !d.idx)) return RZ_ERR_INVALID_ARG;
+        if (!list_aligned(d, w)) return RZ_ERR_INVALID_ARG;
         ListRec r{};
         r.data = static_cast<uint8_t*>(d.data);
         r.idx = d.idx;
@@ -641,6 +649,8 @@ int arena_launch(BatchArena* a, const rz_list_desc* lists, int nlists, cudaStrea
     for (int l = 0; l < nlists; ++l) {
         const rz_list_desc& d = lists[l];
         if (d.n < 0 || d.k < 0 || d.k > d.n || d.n >= (int64_t(1) << 32)) return RZ_ERR_INVALID_ARG;
+        if (d.k > 0 && (!d.data || !d.idx)) return RZ_ERR_INVALID_ARG;
+        if (!list_aligned(d, a->w)) return RZ_ERR_INVALID_ARG;
         if (d.k == 0 || d.k == d.n) continue;
         const uint32_t nch = uint32_t((uint64_t(d.k) + TILE - 1) / TILE);
         if (nch > kMaxTilesPerList) return RZ_ERR_UNSUPPORTED;

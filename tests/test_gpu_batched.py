@@ -1,4 +1,6 @@
 """GPU parity of the batched (one persistent launch, graph-replayed) path against the oracle."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -106,3 +108,29 @@ def test_batched_large_lists_with_many_chunks(ctx):
     for l, exp in enumerate(expected(hosts, idxs)):
         n, k = exp.shape[0], idxs[l].size
         assert np.array_equal(dl[l][0].cpu().numpy().view(np.uint32)[: n - k], exp[: n - k]), l
+
+
+def test_batched_rejects_misaligned_lists(ctx):
+    """A list whose items are not aligned to their width (or whose index list is not 4-byte
+    aligned) is refused on the host with RZ_ERR_INVALID_ARG before anything is launched, and
+    the context stays usable."""
+    raw = torch.zeros(4096 * 2 + 2, dtype=torch.int32, device=DEV)
+    idx = torch.arange(0, 4096, 4, dtype=torch.int32, device=DEV)
+    arr = (_native.ListDesc * 1)()
+    arr[0].data = raw.data_ptr() + 4  # 8-byte items at a 4-byte offset
+    arr[0].idx = idx.data_ptr()
+    arr[0].n = 4096
+    arr[0].k = idx.numel()
+    plan = ctypes.c_void_p()
+    st = _native.lib.rz_batch_plan_create(ctx.handle, arr, 1, 8, None, ctypes.byref(plan))
+    assert st == _native.RZ_ERR_INVALID_ARG
+    hosts, idxs = make_lists(3, 8, 10, 14, 2)
+    lists = to_dev(hosts, idxs)
+    plan = rz.BatchPlan(ctx, lists)
+    plan.launch()
+    torch.cuda.synchronize()
+    assert ctx.sync_status() == 0
+    for (d, _), e, i in zip(lists, expected(hosts, idxs), idxs):
+        n, k = d.shape[0], i.size
+        assert np.array_equal(d.cpu().numpy().view(np.uint32)[: n - k], e[: n - k])
+    plan.close()
