@@ -316,8 +316,8 @@ typedef struct rz_batch_plan rz_batch_plan;
  * its work queue and scratch. cfg == NULL uses the configuration the list-mix predictor picks
  * when one is attached (rz_set_batch_predictor; only configurations whose tile lets the longest
  * list fit in 1024 tiles are candidates), else the context's tuned batched configuration, else the
- * built-in default (512 x 4 x 4, wavefront order; 256 x 8 x 4 phase by phase for 32-byte items),
- * its tile raised until the longest list fits.
+ * built-in default (512 x 4 x 4, wavefront order; 256 x 4 x 4 for 32-byte items), its tile
+ * raised until the longest list fits.
  * An explicit configuration whose tile is too small for a list fails with RZ_ERR_UNSUPPORTED.
  * Each list's result equals rz_remove on that list (the reference's per-list calls,
  * redzone.hxx:1089-1166, one launch each).

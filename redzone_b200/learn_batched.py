@@ -76,9 +76,9 @@ MAX_TILES_PER_LIST = 1024  # a list of the batched kernel spans at most this man
 
 def default_cfg(w: int, kmax: int = 0) -> tuple[int, int, int, int]:
     """The configuration rz_batch_plan_create uses without a predictor or table: 512 x 4 x 4 CTAs
-    per SM in wavefront order (256 x 8 x 4 phase by phase for 32-byte items), with items and then
-    block raised until the longest list (kmax removals) fits the tile limit."""
-    block, items, wave = (256, 8, 0) if w >= 32 else (512, 4, DEFAULT_WAVE)
+    per SM in wavefront order (256 x 4 x 4 for 32-byte items), with items and then block raised
+    until the longest list (kmax removals) fits the tile limit."""
+    block, items, wave = (256 if w >= 32 else 512), 4, DEFAULT_WAVE
     while block * items * MAX_TILES_PER_LIST < kmax:
         if items < 8:
             items *= 2

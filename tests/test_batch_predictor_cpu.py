@@ -35,7 +35,7 @@ def test_batch_config_space():
     assert {wv for _, _, _, wv in space} == {0, learn_batched.DEFAULT_WAVE}
     for w in (4, 8, 16):
         assert space[learn_batched.default_class(None, w)] == (512, 4, 4, learn_batched.DEFAULT_WAVE)
-    assert space[learn_batched.default_class(None, 32)] == (256, 8, 4, 0)
+    assert space[learn_batched.default_class(None, 32)] == (256, 4, 4, learn_batched.DEFAULT_WAVE)
 
 
 def test_soft_targets_ignore_infeasible_configurations():
