@@ -426,7 +426,7 @@ def own_arm(args):
     e_pinned = [torch.from_numpy(s.astype(np.int32)).pin_memory() for s in e_np]
     for i in range(max(args.warmup, E_DEPTH + 1)):  # first use grows the staging slots
         assert ctx.wait(ctx.remove_host_idx_async(a, e_pinned[i % E_SETS])) == n - k
-    e_steps = max(args.steps, 50)
+    e_steps = max(args.steps, 1000)  # the 6-deep pipeline fills and drains once per region
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
