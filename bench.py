@@ -19,7 +19,7 @@ Also reported on the same line:
     scrub between steps);
   * end to end (e2e): the pipelined host-index call (rz_remove_host_idx_async / rz_wait) from C++
     (redzone_b200/_lib/rz_e2e) and from Python, each step copying its removal list from pinned
-    host memory and receiving its new length (and status bits, on failure) from the kernel;
+    host memory and reading its status and new length back;
   * the batched half of the metric: 4096 uneven lists in one launch with the configuration the
     learned list-mix predictor picks, against per-list launches, the default configuration, an
     exhaustive autotune of the configuration space, and the hole writes alone;
@@ -54,8 +54,8 @@ NSETS = 8
 SCRUB_BYTES = 256 << 20
 FALLBACK_HBM_GBS = 6650.0
 
-# Device -> host per pipelined call at this workload: the kernel writes {ticket, new length} into
-# mapped pinned memory (16 bytes; status bits follow only when a call fails).
+# Device -> host per pipelined call: the call's status word and device-tracked length, read back
+# as one 16-byte copy.
 RESULT_BYTES = 16
 METRIC = "items removed/s"
 UNIT = "items/s"
@@ -526,9 +526,9 @@ def own_arm(args):
                 "value": world * k / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 4 * k,
                 "d2h_bytes_per_step": RESULT_BYTES, "ms_per_step": e2e_ms, "steps": e_steps,
                 "method": f"Python (ctypes) caller: rz_remove_host_idx_async, {E_DEPTH} calls in flight, each "
-                          f"step's list copied from pinned host memory, its new length (and status bits, on "
-                          f"failure) written by the kernel into mapped pinned memory, rz_wait on every step; time "
-                          f"of the whole region / steps; {E_SETS} distinct lists, no L2 scrub",
+                          f"step's list copied from pinned host memory and its status + new length read back "
+                          f"(16 bytes), rz_wait on every step; time of the whole region / steps; {E_SETS} "
+                          f"distinct lists, no L2 scrub",
                 "serial_ms_per_step": e2e_serial_ms, "host_issue_us_per_call": 1e6 * issue_s / e_steps}),
             "cpu_baseline": cpu,
             "batched": bat,
@@ -551,9 +551,9 @@ def e2e_line(k: int, world: int, cpp: dict | None, py: dict) -> dict:
             "ms_per_step": cpp["ms_per_step"], "steps": cpp["steps"],
             "method": f"C++ caller through the C-ABI (redzone_b200/_lib/rz_e2e): rz_remove_host_idx_async, "
                       f"{cpp['depth']} calls in flight, each step's list copied from pinned host memory and its "
-                      f"new length (and status bits, on failure) written by the kernel into mapped pinned "
-                      f"memory, rz_wait on every step (status and length checked); CUDA events around the "
-                      f"whole region / steps; {cpp['sets']} distinct lists, no L2 scrub",
+                      f"status + new length read back (16 bytes), rz_wait on every step (status and length "
+                      f"checked); CUDA events around the whole region / steps; {cpp['sets']} distinct lists, "
+                      f"no L2 scrub",
             "serial_ms_per_step": cpp["serial_ms_per_step"], "host_issue_us_per_call": cpp["host_issue_us_per_call"],
             "python": py}
 

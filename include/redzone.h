@@ -127,12 +127,9 @@ int rz_remove_host_idx(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem_bytes
  * Pipelined form of rz_remove_host_idx for a host program that hands the GPU one removal list
  * after another (redzone_CPU, Redzone_CPU.hxx:150, called in a loop): returns without waiting.
  * The index list is copied on the context's own copy stream, so the copy of one call overlaps
- * the kernel of the one before; the removal runs on `stream` after its copy. The call's result
- * comes back without a copy of its own where the removal kernel can hand it over (the default
- * schedules for k <= 2^17): the kernel writes the new length into pinned host memory as it
- * starts, and the status bits of a failed call as it ends; for other schedules the status and
- * device-tracked length are read back on a third stream while the next removal runs. *ticket
- * names the call for rz_wait. h_idx (ideally pinned) must stay
+ * the kernel of the one before; the removal runs on `stream` after its copy; the call's own
+ * status and device-tracked length (16 bytes) are read back into pinned memory on a third stream
+ * while the next removal runs. *ticket names the call for rz_wait. h_idx (ideally pinned) must stay
  * unchanged until rz_wait for the call returns. Calls are ordered on `stream` as issued. Up to 8
  * calls per context are in flight; issuing a 9th waits for the oldest (its result is kept for
  * rz_wait). The staging buffers grow to the largest k seen (context scratch). Each call reports

@@ -112,30 +112,6 @@ __device__ __forceinline__ void st_hint(u32x8* a, const u32x8& v, uint64_t pol) 
     st_hint(&a->b, v.b, pol);
 }
 
-// ---- result hand-off of a pipelined host-index call (PublishArgs) ----------------------------
-// publish_length: thread 0 of CTA 0 writes {ticket, new length} into the result words with one
-// 16-byte store at the start of the kernel, where the PCIe write has long completed by the time
-// the CTA ends. publish_result: called by every thread of a CTA, once, after the CTA's last write
-// to the status word, on every exit path of the kernel. Thread 0 reads the status word after the
-// CTA barrier, so it holds every bit this CTA set and every bit set before the kernel; for each
-// bit set it stores 1 into that bit's host word (idempotent: what all CTAs report together is
-// the union of their bits). A call without errors writes nothing more to host memory: a write
-// at the end would hold the CTA until the PCIe write is acknowledged.
-__device__ __forceinline__ void publish_length(const PublishArgs& pb, unsigned long long len) {
-    if (pb.host == nullptr || blockIdx.x != 0 || threadIdx.x != 0) return;
-    asm volatile("st.global.volatile.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(pb.host + kPubResultWord),
-                 "r"(pb.ticket), "r"(uint32_t(len)), "r"(uint32_t(len >> 32)), "r"(0u)
-                 : "memory");
-}
-__device__ __forceinline__ void publish_result(const PublishArgs& pb, const uint32_t* status) {
-    if (pb.host == nullptr) return;  // uniform: a kernel parameter
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    const uint32_t st = *reinterpret_cast<const volatile uint32_t*>(status);
-    for (uint32_t b = 0; b < 32u && (st >> b); ++b)
-        if ((st >> b) & 1u) reinterpret_cast<volatile uint32_t*>(pb.host)[b] = 1u;
-}
-
 // ---- epoch-tagged arrival flags --------------------------------------------------------------
 // The grid schedule's barriers. Each call reads an epoch E once at kernel start and tags every
 // arrival with E+1; a CTA arrives with one release store to its own slot and waits by polling the

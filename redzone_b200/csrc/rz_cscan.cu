@@ -50,7 +50,6 @@ struct CscanParams {
     unsigned long long* dev_len;
     unsigned long long* stamps;  // nullable: 8 globaltimer stamps per CTA
     uint32_t validate;
-    PublishArgs pub;             // pipelined host-index call: result hand-off (else host == nullptr)
 };
 
 // Dynamic shared memory: the pairing layout of rz_pairfill.cuh (full V and P maps, the slow
@@ -103,7 +102,6 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
     const uint32_t n = p.n, k = p.k, cut = n - k;
     const int B = blockDim.x, nw = B >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t q = cluster.block_rank();
-    publish_length(p.pub, (unsigned long long)(n - k));
 
     // ---- the critical path starts with this CTA's slice of the index list: issue it first ------
     // Slices are multiples of 4 entries (16-byte aligned); warp w of CTA q reads entries
@@ -179,7 +177,6 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
         cluster_wait();
         cluster_arrive();
         cluster_wait();
-        publish_result(p.pub, p.status);
         return;
     }
     CS_STAMP(1);
@@ -297,7 +294,6 @@ __global__ void __launch_bounds__(MAXB, 1) redzone_cscan_kernel(const CscanParam
 #pragma unroll
         for (int i = 0; i < 8; ++i) p.stamps[blockIdx.x * kStampsPerCta + i] = st_[i];
     }
-    publish_result(p.pub, p.status);
 }
 
 using CscanFn = void (*)(const CscanParams);
@@ -400,7 +396,6 @@ int launch_cscan(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t
     p.dev_len = ctx->ws.dev_len;
     p.stamps = ctx->ws.stamps_on ? ctx->ws.stamps : nullptr;
     p.validate = validate ? 1u : 0u;
-    p.pub = ctx->pub;
 
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3(grid);
@@ -416,7 +411,6 @@ int launch_cscan(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32_t
     lc.numAttrs = 1;
     if (!cscan_cluster_fits(ctx, f, &lc)) return RZ_ERR_UNSUPPORTED;
     RZ_CUDA_TRY(ctx, cudaLaunchKernelEx(&lc, f, p));
-    if (p.pub.host) ctx->pub_used = true;
     if (info) {
         info->grid = int(grid);
         info->block = block;

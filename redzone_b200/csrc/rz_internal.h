@@ -59,18 +59,6 @@ struct Workspace {
     bool dirty = false;
 };
 
-// Result hand-off of a pipelined host-index call (rz_async.cpp). `host` is mapped pinned memory:
-// words [0, 32) one per status bit (zero on entry), words [kPubResultWord, +4) the result
-// {ticket, new length lo, new length hi, 0}. A kernel given `host` writes the result words once
-// (CTA 0, at its start) and sets word b to 1 when status bit b is set at the end of any of its
-// CTAs. host == nullptr (every other launch): nothing is written.
-constexpr uint32_t kPubResultWord = 32;
-constexpr uint32_t kPubWords = kPubResultWord + 4;
-struct PublishArgs {
-    uint32_t* host = nullptr;
-    uint32_t ticket = 0;
-};
-
 }  // namespace rz
 
 struct rz_ctx {
@@ -89,8 +77,6 @@ struct rz_ctx {
     size_t scratch_held = 0;     // bytes of grown context scratch
     size_t scratch_limit = ~size_t(0);  // rz_set_scratch_limit: growth beyond it -> RZ_ERR_NO_MEMORY
     cudaEvent_t done_event = nullptr;    // completion of a synchronous call's last copy (polled)
-    rz::PublishArgs pub;         // set by the pipelined host-index call around its launch
-    bool pub_used = false;       // a launcher passed `pub` to the kernel it launched
 };
 
 namespace rz {

@@ -67,7 +67,6 @@ struct ProducedParams {
     uint32_t validate;
     uint32_t pdl;                // wait for the preceding (scan) grid before reading candidates
     uint32_t full_scan;          // scan-all schedule: every CTA reads the whole (16-byte aligned) list
-    PublishArgs pub;             // pipelined host-index call: result hand-off (else host == nullptr)
 };
 
 template <int W, int IPT>
@@ -77,19 +76,13 @@ __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(con
     const uint32_t n = p.n;
     if (k > p.capacity) {  // uniform: every CTA reads the same counts
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(p.status, ST_CAPACITY);
-        publish_length(p.pub, (unsigned long long)n);  // nothing moved
-        publish_result(p.pub, p.status);
         return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && p.dev_len) *p.dev_len = (unsigned long long)(n - k);
-    publish_length(p.pub, (unsigned long long)(n - k));
     const uint32_t B = blockDim.x, TILE = B * IPT;
     const uint32_t ntiles = (k + TILE - 1) / TILE;
     const uint32_t t = blockIdx.x;
-    if (t >= ntiles || k == n) {  // no tile here, or nothing survives (nothing moves)
-        publish_result(p.pub, p.status);
-        return;
-    }
+    if (t >= ntiles || k == n) return;  // no tile here, or nothing survives (nothing moves)
     const uint32_t cut = n - k, kw = (k + 31) >> 5, kwc = (p.capacity + 31) >> 5;
     const uint32_t chunk_base = t * TILE;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = int(B >> 5);
@@ -143,10 +136,7 @@ __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(con
         }
     }
     __syncthreads();
-    if (s_abort) {  // validation failed: nothing moves
-        publish_result(p.pub, p.status);
-        return;
-    }
+    if (s_abort) return;  // validation failed: nothing moves
     const uint32_t m = s_m;
 
     // ---- the red entries: from the candidates, or (candidates overflowed) from the whole list ---
@@ -265,7 +255,6 @@ __global__ void __launch_bounds__(kProducedBlock, 1) redzone_produced_kernel(con
     uint32_t stot, dbase;
     derive_pairing<IPT>(pf, R, k, chunk_base, true, p.status, stot, dbase);
     fill_holes<W, IPT>(pf, R, k, cut, chunk_base, stot, dbase, rr, src, head, tail);
-    publish_result(p.pub, p.status);
 }
 
 using ProducedFn = void (*)(const ProducedParams);
@@ -477,10 +466,8 @@ int launch_scanall(rz_ctx* ctx, void* data, uint32_t n, uint32_t w, const uint32
     pp.validate = validate ? 1u : 0u;
     pp.pdl = 0;
     pp.full_scan = 1;
-    pp.pub = ctx->pub;
     f<<<grid, kProducedBlock, smem, s>>>(pp);
     RZ_CUDA_TRY(ctx, cudaGetLastError());
-    if (pp.pub.host) ctx->pub_used = true;
     if (info) {
         info->grid = int(grid);
         info->block = kProducedBlock;
