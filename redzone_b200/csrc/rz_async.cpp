@@ -11,8 +11,10 @@
 //   copy stream : H2D h_idx -> slot.d_idx ; record slot.copied
 //   call stream : wait slot.copied ; [zero slot.status, after a call that reported an error] ;
 //                 removal kernel(s) ; record slot.kdone
-//   read stream : wait slot.kdone ; D2H slot.status|length (16 bytes) -> slot.h_res ;
+//   read stream : wait slot.kdone ; D2H slot.status|flag|length (16 bytes) -> slot.h_res ;
 //                 record slot.done
+// rz_wait spins on the landing flag (a word that is zero on the device and armed on the host)
+// instead of querying the event: no CUDA call per wait (the event remains the fallback).
 // The index copy of call i+1 runs while call i's kernel runs, and call i's read-back while call
 // i+1's kernel runs, so with a few calls in flight the call stream runs the kernels back to back.
 // The read-back is one 16-byte copy and nothing else: measured on B200 with a 256 KB list per
@@ -24,6 +26,8 @@
 // issues more than kSlots calls ahead, after the issuing call has waited for it and kept its
 // result for a later rz_wait.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstring>
 #include <deque>
 #include <new>
@@ -37,7 +41,9 @@ namespace {
 constexpr int kSlots = 8;
 constexpr size_t kStashMax = 1024;  // results of calls evicted from their slot before rz_wait
 constexpr size_t kSlotResBytes = 256;   // a slot's device status (offset 0) and length (offset 8)
-constexpr size_t kSlotReadBytes = 16;   // what comes back per call: status word, pad, length
+constexpr size_t kSlotReadBytes = 16;   // what comes back per call: status word, landing flag, length
+constexpr uint32_t kArmed = 0xffffffffu;  // the host's landing flag before the read-back arrives
+constexpr auto kLandPoll = std::chrono::microseconds(2000);
 
 struct Slot {
     uint32_t* d_idx = nullptr;
@@ -117,8 +123,21 @@ int pipe_create(rz_ctx* ctx, AsyncPipe** out) {
 // device error marks the context scratch for a reset before its next call, and the slot's status
 // word for clearing before the slot's next call.
 int collect(rz_ctx* ctx, Slot& s, Result* r) {
-    const int st = wait_event(ctx, s.done);
-    if (st != RZ_OK) return st;
+    // The read-back copies 16 bytes whose word at offset 4 is zero on the device; the host set its
+    // copy of that word to kArmed when it issued the call, so zero there means the copy has landed
+    // (one 16-byte write). Spin on it for up to kLandPoll, then wait for the slot's event.
+    volatile const uint32_t* flag = reinterpret_cast<volatile const uint32_t*>(s.h_res + 4);
+    bool landed = *flag == 0u;
+    if (!landed) {
+        const auto t0 = std::chrono::steady_clock::now();
+        while (!(landed = (*flag == 0u)) && std::chrono::steady_clock::now() - t0 < kLandPoll) {
+        }
+    }
+    if (!landed) {
+        const int st = wait_event(ctx, s.done);
+        if (st != RZ_OK) return st;
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
     uint32_t bits = 0;
     unsigned long long len = 0;
     std::memcpy(&bits, s.h_res, sizeof(bits));
@@ -234,6 +253,7 @@ int rz_remove_host_idx_async(rz_ctx* ctx, void* d_data, int64_t n, uint32_t elem
     RZ_CUDA_TRY(ctx, cudaEventRecord(s.kdone, cs));
     // Read stream: the result comes back while the call stream runs the next removal.
     RZ_CUDA_TRY(ctx, cudaStreamWaitEvent(P.read_stream, s.kdone, 0));
+    *reinterpret_cast<volatile uint32_t*>(s.h_res + 4) = kArmed;
     RZ_CUDA_TRY(ctx, cudaMemcpyAsync(s.h_res, s.d_res, kSlotReadBytes, cudaMemcpyDeviceToHost, P.read_stream));
     RZ_CUDA_TRY(ctx, cudaEventRecord(s.done, P.read_stream));
     s.ticket = t;
