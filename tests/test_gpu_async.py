@@ -130,10 +130,9 @@ def test_async_errors_stay_with_their_call(ctx):
 @pytest.mark.parametrize("k", [1 << 10, 1 << 14, 1 << 18])
 def test_async_error_reports_and_slot_reuse(ctx, k):
     """An out-of-range index in one call comes back from that call's rz_wait, whichever kernel ran
-    (scan-all at 2^10, cluster scan at 2^14 -- both hand their result over from the kernel -- and
-    the grid schedule at 2^18, which uses the read-back copy), and the calls issued after it on
-    the same staging slots report success with the canonical result: the slot's status word
-    starts clean again."""
+    (scan-all at 2^10, cluster scan at 2^14, the grid schedule at 2^18), and the calls issued
+    after it on the same staging slots report success with the canonical result: the slot's
+    status word, cleared on the call stream after the error, starts clean again."""
     n = 1 << 21
     calls = 20
     lists = [workloads.uniform(n, k, seed=500 + j).astype(np.int64) for j in range(calls)]
@@ -162,8 +161,8 @@ def test_async_error_reports_and_slot_reuse(ctx, k):
 @pytest.mark.parametrize("k", [1 << 10, 1 << 14])
 def test_async_validation_abort_reports_duplicate(ctx, k):
     """A repeated index under RZ_VALIDATE stops the removal kernel before it moves anything
-    (scan-all at 2^10, cluster scan at 2^14: both report from the kernel's abort path), rz_wait
-    returns RZ_ERR_DUPLICATE, the array is untouched, and the next call on the context succeeds."""
+    (scan-all at 2^10, cluster scan at 2^14: each kernel's own abort path), rz_wait returns
+    RZ_ERR_DUPLICATE, the array is untouched, and the next call on the context succeeds."""
     n = 1 << 20
     good = workloads.uniform(n, k, seed=90 + k).astype(np.int32)
     bad = good.copy()
