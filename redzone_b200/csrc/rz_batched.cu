@@ -32,6 +32,7 @@ namespace rz {
 enum : uint32_t { K_MARK = 0, K_SINGLE = 1, K_CLASSIFY = 2, K_PAIR = 3 };
 constexpr uint32_t kMaxTilesPerList = kBatchMaxTilesPerList;
 constexpr uint32_t kNoItem = 0xffffffffu;
+constexpr int kMarkLoads = 8;   // index loads in flight per thread in a MARK item
 
 struct ListRec {            // one per list, device-resident
     uint8_t* data;
@@ -169,18 +170,22 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
         const uint32_t t_begin = grp * L.span, t_end = min(t_begin + L.span, L.nch);
 
         if (kind == K_MARK) {
-            for (uint32_t c = t_begin; c < t_end; ++c) {
-                const uint32_t base = c * TILE;
-                if (c + 1 < t_end) prefetch_l2(L.idx + base + TILE, size_t(min(TILE, k - base - TILE)) * 4);
+            // The group's index entries in any order, kMarkLoads loads in flight per thread:
+            // marking waits on index bytes in flight, not on its (fire-and-forget) atomics.
+            const uint32_t lo = t_begin * TILE, hi = min(t_end * TILE, k);
+            for (uint32_t b = lo + threadIdx.x; b < hi; b += uint32_t(kMarkLoads) * B) {
+                uint32_t r[kMarkLoads];
 #pragma unroll
-                for (int j = 0; j < IPT; ++j) {
-                    const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
-                    if (i < k) {
-                        const uint32_t r = __ldg(&L.idx[i]);
-                        if (r >= cut) {
-                            if (r >= n) atomicOr(p.status, ST_RANGE);
-                            else atomicOr(&p.bitmap[L.bitmap_off + ((r - cut) >> 5)], 1u << ((r - cut) & 31u));
-                        }
+                for (int j = 0; j < kMarkLoads; ++j) {
+                    const uint32_t i = b + uint32_t(j) * B;
+                    r[j] = i < hi ? __ldg(&L.idx[i]) : 0u;
+                }
+#pragma unroll
+                for (int j = 0; j < kMarkLoads; ++j) {
+                    const uint32_t i = b + uint32_t(j) * B;
+                    if (i < hi && r[j] >= cut) {
+                        if (r[j] >= n) atomicOr(p.status, ST_RANGE);
+                        else atomicOr(&p.bitmap[L.bitmap_off + ((r[j] - cut) >> 5)], 1u << ((r[j] - cut) & 31u));
                     }
                 }
             }
