@@ -52,6 +52,8 @@ __host__ __device__ inline size_t redlist_smem_bytes(uint32_t k) {
     return (size_t(2) * ((k + 31) / 32) + size_t(3) * kFastMaxRed) * 4;
 }
 
+constexpr uint32_t kDeepMarkLoads = 8;  // phase A index loads in flight per thread (several tiles per CTA)
+
 // ------------------------------------------------------------------------------------------------
 // Redzone, one list, G persistent CTAs (G == 1 degenerates to block-level synchronisation).
 // ------------------------------------------------------------------------------------------------
@@ -95,25 +97,59 @@ __device__ __forceinline__ void redzone_single_body(const SingleParams& p) {
 
     // ---- phase A: mark the red zone ---------------------------------------------------------
     // The loads are issued before the first __syncthreads so they overlap the epoch read.
-    for (uint32_t t = t0; t < t1; ++t) {
-        const uint32_t base = t * TILE;
+    // Several tiles per CTA: the CTA's index entries in any order, kDeepMarkLoads loads in flight
+    // per thread (a mark needs nothing but its own entry; phase B re-reads the indices).
+    if (!single && t0 < t1) {
+        constexpr uint32_t U = kDeepMarkLoads;
+        const uint32_t hi = min(t1 * TILE, k), step = U * uint32_t(B);
+        uint32_t b = t0 * TILE + threadIdx.x;
+        uint32_t r[U];
+#pragma unroll
+        for (uint32_t j = 0; j < U; ++j) {
+            const uint32_t i = b + j * B;
+            r[j] = (i < hi) ? __ldg(&p.idx[i]) : 0u;
+        }
+        __syncthreads();  // s_abort / s_tag
+        if (s_abort) return;  // validation failed: leave the caller's data untouched
+        for (;;) {
+#pragma unroll
+            for (uint32_t j = 0; j < U; ++j) {
+                const uint32_t i = b + j * B;
+                if (i < hi && r[j] >= cut) {
+                    if (r[j] >= n) {
+                        atomicOr(p.status, ST_RANGE);
+                    } else {
+                        const uint32_t off = r[j] - cut;
+                        const uint32_t bit = 1u << (off & 31u);
+                        if (p.validate) {
+                            if (atomicOr(&p.bitmap[off >> 5], bit) & bit) atomicOr(p.status, ST_DUPLICATE);
+                        } else {
+                            atomicOr(&p.bitmap[off >> 5], bit);
+                        }
+                    }
+                }
+            }
+            if (b >= hi || hi - b <= step) break;
+            b += step;
+#pragma unroll
+            for (uint32_t j = 0; j < U; ++j) {
+                const uint32_t i = b + j * B;
+                r[j] = (i < hi) ? __ldg(&p.idx[i]) : 0u;
+            }
+        }
+    }
+    if (single && t0 < t1) {  // one tile: its indices stay in registers for phase B
+        const uint32_t base = t0 * TILE;
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
             rr[j] = (i < k) ? __ldg(&p.idx[i]) : 0xffffffffu;
         }
-        if (single) {
-            // Pull this CTA's tail window into L2 while the grid waits at the barrier. A prefetch
-            // is not an outstanding access the arrival's release has to wait for (a load is).
-            const uint32_t cnt = min(TILE, k - base);
-            prefetch_l2(tail + base, size_t(cnt) * W);
-        } else if (t + 1 < t1) {
-            prefetch_l2(p.idx + base + TILE, size_t(min(TILE, k - base - TILE)) * 4);  // next tile
-        }
-        if (t == t0) {
-            __syncthreads();  // s_abort / s_tag
-            if (s_abort) return;  // validation failed: leave the caller's data untouched
-        }
+        // Pull this CTA's tail window into L2 while the grid waits at the barrier. A prefetch
+        // is not an outstanding access the arrival's release has to wait for (a load is).
+        prefetch_l2(tail + base, size_t(min(TILE, k - base)) * W);
+        __syncthreads();  // s_abort / s_tag
+        if (s_abort) return;  // validation failed: leave the caller's data untouched
 #pragma unroll
         for (int j = 0; j < IPT; ++j) {
             const uint32_t i = base + uint32_t(j) * B + threadIdx.x;
