@@ -247,6 +247,30 @@ def test_validation_on_the_cluster_scan_and_split_schedules(ctx, sched):
     assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
 
 
+@pytest.mark.parametrize("block,items", [(128, 1), (256, 2)])
+def test_validation_on_the_grid_schedule_with_many_tiles_per_cta(ctx, block, items):
+    """The grid schedule with several tiles per CTA (its marking walks each CTA's whole index
+    range at once): a duplicate or an out-of-range index under RZ_VALIDATE is reported and leaves
+    the data untouched, and the next calls, validated or not, on a ragged k (no whole last tile)
+    give the exact result."""
+    n, k = 1 << 20, (1 << 17) + 77
+    host = payload(n, 1, seed=21)
+    idx = workloads.uniform(n, k, seed=21)
+    cfg = rz.LaunchCfg(block, items, 1, 0, SCHEDULES["grid"])
+    for bad_at, bad_val, code in ((k - 5, None, 2), (k // 2, n + 3, 3)):
+        bad = idx.copy()
+        bad[bad_at] = bad[bad_at - 1000] if bad_val is None else bad_val
+        d = torch.from_numpy(host.view(np.int32).copy()).to(DEV)
+        with pytest.raises(rz.RedzoneError) as e:
+            ctx.remove_cfg(d, torch.from_numpy(bad.astype(np.int32)).to(DEV), cfg, flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+        assert e.value.code == code
+        assert np.array_equal(d.cpu().numpy().view(np.uint32), host)
+    got = run_gpu(ctx, host, idx, cfg=cfg, flags=rz.RZ_VALIDATE | rz.RZ_SYNC)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+    got = run_gpu(ctx, host, idx, cfg=cfg)
+    assert np.array_equal(got[: n - k], expect_of(host, idx)[: n - k])
+
+
 def test_out_of_range_without_validation_is_memory_safe(ctx):
     """Bad indices never cause out-of-bounds accesses: an index >= n is ignored, reported."""
     n, k = 1 << 14, 512
