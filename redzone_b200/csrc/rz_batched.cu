@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
     uint32_t* s_bits = smem;
     uint32_t* s_dl = smem + TILE / 32;
     uint32_t* s_sl = s_dl + TILE;
-    __shared__ uint32_t s_cnt[8 * 32 + 1];
+    __shared__ uint32_t s_cnt[2][8 * 32 + 1];  // rank counts; CLASSIFY alternates them between tiles
     __shared__ uint32_t s_item[2];
     __shared__ int s_ok;
     __shared__ uint32_t s_pfx[2 * kMaxTilesPerList + 2];  // PAIR: per-tile prefixes of D and S
@@ -237,9 +237,9 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
 #pragma unroll
             for (int j = 0; j < IPT; ++j)
                 if (dv[j] && sv[j]) st_hint(head + rr[j], src[j], pol_hole);
-            const uint32_t tot = rank_orphans<IPT>(dv, sv, dmask, smask, s_cnt);
+            const uint32_t tot = rank_orphans<IPT>(dv, sv, dmask, smask, s_cnt[0]);
             if (tot != 0u) {
-                write_orphans<IPT>(dv, sv, dmask, smask, rr, s_cnt, 0, cut, s_dl, s_sl);
+                write_orphans<IPT>(dv, sv, dmask, smask, rr, s_cnt[0], 0, cut, s_dl, s_sl);
                 __syncthreads();
                 const uint32_t dcnt = tot >> 16, scnt = tot & 0xffffu;
                 const uint32_t m = min(dcnt, scnt);
@@ -302,16 +302,20 @@ __global__ void __launch_bounds__(512, batched_min_blocks<W, IPT>()) redzone_bat
                         if (i < k) p.bitmap[L.bitmap_off + (i >> 5)] = 0u;  // leave the bitmap zero
                     }
                 }
-                const uint32_t tot = rank_orphans<IPT>(dv, sv, dmask, smask, s_cnt);
+                // Alternate count buffers: tile c + 1 writes the other one, and tile c + 2 writes
+                // this one only after every thread has passed tile c + 1's barriers, i.e. after
+                // every read of this tile's counts.
+                uint32_t* cnt = s_cnt[c & 1u];
+                const uint32_t tot = rank_orphans<IPT>(dv, sv, dmask, smask, cnt);
                 if (tot != 0u)
-                    write_orphans<IPT>(dv, sv, dmask, smask, rr, s_cnt, base, cut,
+                    write_orphans<IPT>(dv, sv, dmask, smask, rr, cnt, base, cut,
                                        p.dlist + L.list_off + base, p.slist + L.list_off + base);
                 if (threadIdx.x == 0) {
                     p.chunk_cnt[L.cnt_off + c] = tot >> 16;
                     p.chunk_cnt[L.cnt_off + L.nch + c] = tot & 0xffffu;
                 }
-                __syncthreads();  // s_cnt is rewritten by the next tile
             }
+            __syncthreads();  // every thread's hole, list and count stores precede the release
             if (threadIdx.x == 0) {
                 __threadfence();
                 atomicAdd(classify_done, 1u);
