@@ -295,7 +295,7 @@ typedef struct rz_list_desc {
 
 /* Tile and schedule of the batched kernel: tile = block * items; lists with k <= tile run whole
  * in one CTA, longer lists are split into tiles and handed out `span` tiles per work item
- * (0 = automatic: up to 8, at least ~32 items per list); ctas_per_sm sets the persistent grid. */
+ * (0 = automatic: 4); ctas_per_sm sets the persistent grid. */
 typedef struct rz_batch_cfg {
     int32_t block;
     int32_t items;

@@ -60,11 +60,12 @@ bool tuned_cfg(rz_ctx* ctx, uint32_t n, uint32_t k, uint32_t w, rz_launch_cfg* c
     return true;
 }
 
-// The best fixed configuration of the batched kernel over 1,000 timed list mixes on B200 (mean
-// regret against exhaustive autotune): 512 x 4 x 4, wavefront order, for items of up to 16 bytes
-// (7.7-9.2 % at 4 and 8 bytes, 4 % at 16). For 32-byte items 256 x 4 x 4, wavefront order: the
-// streaming service's records (2^27 x 32 bytes) sustain 4.45e9 rows/s with it against 4.13e9
-// with 256 x 8 x 4 phase by phase, the best fixed choice on the timed mixes.
+// The best fixed configuration of the batched kernel over 1,000 timed list mixes on B200:
+// 512 x 4 x 4, wavefront order, for items of up to 16 bytes (7.1 % mean regret against
+// exhaustive autotune on the 100 held-out mixes). For 32-byte items 256 x 4 x 4, wavefront order:
+// the streaming service's records (2^27 x 32 bytes) sustain 4.7e9 rows/s with it, and on an
+// earlier build 4.45e9 against 4.13e9 with 256 x 8 x 4 phase by phase, the best fixed choice on
+// the timed mixes of that build.
 bool default_batch_cfg(const rz_ctx* ctx, uint32_t w, rz_batch_cfg* cfg) {
     cfg->block = 512;
     cfg->items = 4;

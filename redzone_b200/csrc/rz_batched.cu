@@ -388,11 +388,12 @@ static BatchFn batch_fn(int w, int items) {
     }
 }
 
-// Tiles per work item for a list of `nch` tiles: long lists get up to 8 tiles per item, which
-// amortises the item's dispatch while keeping at least ~32 items per list for load balance.
+// Tiles per work item for a list of `nch` tiles: 4 by default. Measured on B200 against the
+// earlier rule (up to 8 tiles, at least ~32 items per list), both with the default wavefront lag:
+// 5-26 % faster on seven list mixes (4, 8, 16 and 32-byte items, lists of 2^8 to 2^22 items),
+// equal on mixes of lists short enough to be one item either way.
 static uint32_t span_for(uint32_t nch, int32_t cfg_span) {
-    if (cfg_span > 0) return std::min<uint32_t>(uint32_t(cfg_span), nch);
-    return std::max<uint32_t>(1u, std::min<uint32_t>(8u, nch / 32u));
+    return std::min<uint32_t>(cfg_span > 0 ? uint32_t(cfg_span) : 4u, nch);
 }
 
 

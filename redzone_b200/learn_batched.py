@@ -42,7 +42,7 @@ from .learn import N_IN, N_OUT, Mlp, _fp
 DATA = Path(__file__).resolve().parent / "data"
 SCRUB_BYTES = 256 << 20
 MAX_ITEMS = 1 << 28  # a mix holds at most this many items (4x that for the benchmark's own family)
-DEFAULT_WAVE = 6     # the built-in default's work order (kDefaultWave)
+DEFAULT_WAVE = 4     # the built-in default's work order (kDefaultWave)
 
 
 def config_space() -> list[tuple[int, int, int, int]]:
